@@ -1,0 +1,166 @@
+/* period_search_b200 — C ABI of the B200-native convex-inversion period scan.
+ *
+ * Drop-in for the GPU operator interface of the reference application
+ * (ahorek/PeriodSearch, period_search_cuda/period_search/start_CUDA.h) and
+ * for the scan loop of its CPU driver (period_search/period_search_BOINC.cpp).
+ * Plain C types only: pointers, sizes, doubles and ints.  All arrays are
+ * 0-based and dense, owned by the caller, and copied by the callee.
+ *
+ * Threading: a context (ps_ctx) belongs to one host thread at a time;
+ * separate contexts are independent.  Errors are returned as status codes
+ * (never exit()); ps_last_error() gives a message for the calling thread.
+ */
+#ifndef PERIOD_SEARCH_B200_H
+#define PERIOD_SEARCH_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  PS_ERR_LIMIT (2) and PS_ERR_SINGULAR (4) carry the
+ * reference's exit codes for the same conditions (period_search_BOINC.cpp
+ * :326-327 etc. exit(2); ludcmp.c:23 exit(4)). */
+enum {
+    PS_OK = 0,
+    PS_ERR_IO = 1,          /* input cannot be opened / output cannot be written */
+    PS_ERR_LIMIT = 2,       /* malformed input or a size limit exceeded */
+    PS_ERR_CUDA = 3,        /* CUDA runtime failure (message in ps_last_error) */
+    PS_ERR_SINGULAR = 4,    /* singular ellipsoid-fit matrix (ludcmp) */
+    PS_ERR_ARG = 5,         /* invalid argument */
+    PS_ERR_DEVICE_LOOP = 6  /* a device loop hit its iteration guard */
+};
+
+/* Numerical form of the fit kernels. */
+enum {
+    PS_FORM_FP64 = 0 /* plain FP64, reference operation order (the drop-in) */
+};
+
+/* One output record per trial period, the six values the reference prints
+ * (period_search_BOINC.cpp:926-931), unrounded. */
+typedef struct {
+    double period_h;   /* 24 * best period [h] */
+    double rms;        /* dev_best */
+    double chi2;       /* dev_best^2 * (ndata - 3) */
+    double dark_pct;   /* dark-facet percentage of the best pole */
+    double lambda_deg; /* best pole longitude in [0, 360) */
+    double beta_deg;   /* best pole latitude */
+} ps_record;
+
+/* One LM fit (one trial period, one initial pole). */
+typedef struct {
+    double dev;       /* final rms deviation */
+    double dark;      /* |sum Area*Nor| of the accepted shape */
+    double totarea;   /* sum of the last evaluated facet areas */
+    double period_d;  /* 2 pi / omega [day] */
+    double lambda_deg;
+    double beta_deg;
+    double chisq;
+    int niter;
+    int status;       /* 0, or the gauss_errc code that froze the fit */
+} ps_fit_result;
+
+/* Problem as the reference's host has it after parsing period_search_in
+ * (period_search_BOINC.cpp:277-485), i.e. what CUDAPrepare/CUDAPrecalc/
+ * CUDAStart receive plus the globals they read (l_curves, l_points, in_rel,
+ * weight, l_max, m_max; period_search_cuda/.../period_search_BOINC.cpp
+ * :141-155).  Vectors are already normalised, times already have jd_0
+ * subtracted, sig is the per-lightcurve mean brightness. */
+typedef struct {
+    int n_points;            /* real data points (no convexity rows) */
+    int n_lc;                /* lightcurves (no convexity pseudo-curve) */
+    const int* lc_points;    /* [n_lc] points per lightcurve */
+    const int* lc_relative;  /* [n_lc] 1 = relative (Inrel), 0 = calibrated */
+    const double* tim;       /* [n_points] JD - jd_0 [day] */
+    const double* ee;        /* [n_points*3] unit asteroid->Earth */
+    const double* ee0;       /* [n_points*3] unit asteroid->Sun */
+    const double* brightness;/* [n_points] */
+    const double* sig;       /* [n_points] */
+    const double* weight;    /* [n_points] */
+    double per_start, per_step_coef, per_end; /* header line 1 */
+    int ia_prd;
+    double phi0_rad;         /* initial rotation angle [rad] */
+    double conw;             /* convexity weight as given */
+    int lmax, mmax, nrows;
+    double par[3];           /* phase function a, d, k */
+    int ia_par[3];
+    double cl;               /* initial Lambert coefficient */
+    int ia_cl;
+    double stop_condition;
+    int n_iter_min;
+    double alamda_incr, alamda_start;
+    double jd_min, jd_max;   /* data span (frequency step rule) */
+    double escl;             /* initial size scale (shape guess) */
+} ps_problem_desc;
+
+typedef struct ps_ctx ps_ctx;
+
+/* Parse a period_search_in file and do the host setup of the reference
+ * (period_search_BOINC.cpp:277-485), then open a context on CUDA device
+ * `device` (replaces the parse + CUDAPrepare, start_CUDA.h:2-4). */
+int ps_open_file(const char* path, int device, int form, ps_ctx** out);
+/* Same from in-memory arrays (replaces CUDAPrepare + the host globals). */
+int ps_open(const ps_problem_desc* desc, int device, int form, ps_ctx** out);
+/* Release the context and its device memory (replaces CUDAUnprepare,
+ * start_CUDA.h:14). */
+void ps_close(ps_ctx* ctx);
+
+/* Convexity-weight optimisation pre-pass (replaces CUDAPrecalc,
+ * start_CUDA.h:9-10; period_search_BOINC.cpp:487-715), then the final setup
+ * (:719-802).  Writes the resulting conw_r. */
+int ps_precalc(ps_ctx* ctx, double* conw_r);
+/* Resume path: use a conw_r from a checkpoint and skip the pre-pass
+ * (period_search_cuda/.../period_search_BOINC.cpp:616-629). */
+int ps_set_conw_r(ps_ctx* ctx, double conw_r);
+/* Trial-period count, (int)((f_start - f_end)/f_step) + 1
+ * (period_search_BOINC.cpp:807). */
+int ps_n_periods(const ps_ctx* ctx);
+/* Scan trial periods n_from..n_to (1-based, inclusive) and write one record
+ * each to host memory (replaces CUDAStart, start_CUDA.h:6-7; the caller
+ * formats the lines).  Requires ps_precalc or ps_set_conw_r first. */
+int ps_scan(ps_ctx* ctx, int n_from, int n_to, ps_record* out);
+/* Same, but the records stay on the device: d_out is a device pointer to
+ * (n_to - n_from + 1) records; stream is a cudaStream_t (NULL = default).
+ * Used to time the scan with inputs and outputs resident in HBM. */
+int ps_scan_device(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, void* stream);
+
+/* One LM fit at trial frequency freq [1/day] from initial pole m (1..10)
+ * (period_search_BOINC.cpp:817-920).  cg_out (may be NULL) receives the
+ * final parameter vector (ma values). */
+int ps_fit(ps_ctx* ctx, double freq, int pole, ps_fit_result* out, double* cg_out);
+/* One model evaluation, the reference's mrqcof (mrqcof.c:16-148) at
+ * parameter vector a (ma values): alpha [mfit*mfit], beta [mfit], chi2. */
+int ps_mrqcof(ps_ctx* ctx, const double* a, double* alpha, double* beta, double* chisq);
+/* Model rows after the relative-lightcurve normalisation:
+ * ymod [n_points+3], dyda [(n_points+3)*ma] (row-major). */
+int ps_model(ps_ctx* ctx, const double* a, double* ymod, double* dyda);
+
+/* Sizes: [0] n_points, [1] n_lc (incl. convexity pseudo-curve),
+ * [2] numfac, [3] ncoef, [4] ma, [5] mfit, [6] n_periods.
+ * Scalars: [0] escl, [1] conw_r, [2] freq_start, [3] freq_end,
+ * [4] freq_step. */
+int ps_info(const ps_ctx* ctx, int* ints, double* dbls);
+/* Copy a host-setup array out (names as the oracle's pso_get_array:
+ * "nor", "darea", "dsph", "cg_first", "ia", "tim", "ee", "ee0",
+ * "brightness", "sig", "weight", "at", "af", "ifp").  Returns the element
+ * count or -1. */
+int ps_get_array(const ps_ctx* ctx, const char* name, double* out);
+
+/* Parse + host setup only, no device: for host-side tests on machines
+ * without a GPU.  The handle supports ps_info/ps_get_array/ps_close. */
+int ps_open_host_only(const char* path, ps_ctx** out);
+
+/* Format one record exactly as the reference prints it
+ * ("%.8f  %.6f  %.6f %4.1f %4.0f %4.0f\n", period_search_BOINC.cpp:926-931);
+ * when first_line is nonzero column 4 is conw_line instead of dark_pct.
+ * Returns the number of characters written (excluding the NUL). */
+int ps_format_record(const ps_record* r, int first_line, double conw_line, char* buf, int buflen);
+
+/* Message for the last error on the calling thread ("" if none). */
+const char* ps_last_error(void);
+/* Kernel launches issued by this process so far (all contexts). */
+long long ps_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,676 @@
+// C ABI of the B200 period scan (include/period_search_b200.h): context
+// lifetime, the per-asteroid device tables, the convexity-weight pre-pass
+// and the period scan driver.  Replaces CUDAPrepare / CUDAPrecalc /
+// CUDAStart / CUDAUnprepare (period_search_cuda/period_search/start_CUDA.h)
+// and the period/pole loops of period_search/period_search_BOINC.cpp.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/period_search_b200.h"
+#include "ps_device.hpp"
+#include "ps_host.hpp"
+
+using psb::Problem;
+
+namespace {
+
+thread_local std::string g_err;
+std::atomic<long long> g_launches{0};
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+    g_err = std::string(where) + ": " + cudaGetErrorString(e);
+    return PS_ERR_CUDA;
+}
+
+#define PSB_CUDA(call)                                  \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t count) {
+        if (count <= n) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+    cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
+        cudaError_t e = ensure(v.size() ? v.size() : 1);
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+}  // namespace
+
+struct ps_ctx {
+    Problem prob;
+    int device = 0;
+    int form = PS_FORM_FP64;
+    bool host_only = true;
+    bool rows_ready = false;
+    cudaStream_t stream = nullptr;
+    int sms = 0, blocks_per_sm = 0;
+    psb::DevProblem dp{};
+    // device tables
+    DevBuf<double> d_pts, d_rows, d_fac, d_dsph, d_cpl, d_cfc, d_cfs, d_cgf, d_pole;
+    DevBuf<int> d_lc, d_free, d_queue;
+    DevBuf<double> d_scratch;
+    DevBuf<psb::FitOut> d_fits;
+    DevBuf<ps_record> d_rec;
+    DevBuf<double> d_eval;
+    DevBuf<psb::DevProblem> d_dp;
+    std::vector<int> free_idx;
+};
+
+namespace {
+
+// Stop rule as the reference sets it up per fit (period_search_BOINC.cpp:846-859).
+void stop_rule(Problem& p, int& n_iter_max, double& iter_diff_max, int& n_iter_min) {
+    n_iter_max = 0;
+    iter_diff_max = -1;
+    if (p.stop_condition > 1) {
+        n_iter_max = (int)p.stop_condition;
+        iter_diff_max = 0;
+        p.n_iter_min = 0;  // the reference overwrites its global n_iter_min
+    }
+    if (p.stop_condition < 1) {
+        n_iter_max = psb::kMaxNIter;
+        iter_diff_max = p.stop_condition;
+    }
+    n_iter_min = p.n_iter_min;
+}
+
+int upload_static(ps_ctx* c) {
+    Problem& p = c->prob;
+    cudaStream_t s = c->stream;
+    const int N = p.n_points, F = p.numfac, C = p.ncoef;
+    const int NCB = ((C + 7) / 8) * 8;
+    if (NCB > 64) return fail(PS_ERR_LIMIT, "the FP64 form supports up to 64 shape coefficients (lmax <= 7)");
+    // points SoA: t, ex, ey, ez, e0x, e0y, e0z, alpha
+    std::vector<double> pts((size_t)8 * N);
+    for (int i = 0; i < N; i++) {
+        const double* e = &p.ee[(size_t)i * 3];
+        const double* e0 = &p.ee0[(size_t)i * 3];
+        pts[(size_t)0 * N + i] = p.tim[i];
+        pts[(size_t)1 * N + i] = e[0];
+        pts[(size_t)2 * N + i] = e[1];
+        pts[(size_t)3 * N + i] = e[2];
+        pts[(size_t)4 * N + i] = e0[0];
+        pts[(size_t)5 * N + i] = e0[1];
+        pts[(size_t)6 * N + i] = e0[2];
+        // bright.c:29-30: phase angle from the unit vectors (dot_product.c)
+        const double cos_alpha = e[0] * e0[0] + e[1] * e0[1] + e[2] * e0[2];
+        pts[(size_t)7 * N + i] = std::acos(cos_alpha);
+    }
+    PSB_CUDA(c->d_pts.upload(pts, s));
+    // lightcurves incl. the convexity pseudo-curve
+    const int L = p.n_lc();
+    std::vector<int> lc((size_t)3 * (L + 1) + 1);
+    int* lc_start = lc.data();
+    int* lc_rel = lc.data() + (L + 2);
+    int* lc_npts = lc_rel + (L + 1);
+    lc_start[0] = 0;
+    for (int i = 0; i < L; i++) {
+        lc_start[i + 1] = lc_start[i] + p.lc_points[i];
+        lc_rel[i] = p.lc_rel[i];
+        lc_npts[i] = p.lc_points[i];
+    }
+    lc_start[L + 1] = lc_start[L] + 3;
+    lc_rel[L] = 0;
+    lc_npts[L] = 3;
+    // facets
+    std::vector<double> fac((size_t)F * 4), dsph((size_t)F * NCB, 0.0);
+    int nq = 0;
+    for (int m = 0; m <= p.mmax; m++) nq += p.lmax - m + 1;
+    std::vector<double> cpl((size_t)F * nq), cfc((size_t)F * (p.mmax + 1)), cfs((size_t)F * (p.mmax + 1));
+    const int L1 = p.lmax + 1;
+    for (int f = 0; f < F; f++) {
+        fac[(size_t)f * 4 + 0] = p.nor[(size_t)f * 3 + 0];
+        fac[(size_t)f * 4 + 1] = p.nor[(size_t)f * 3 + 1];
+        fac[(size_t)f * 4 + 2] = p.nor[(size_t)f * 3 + 2];
+        fac[(size_t)f * 4 + 3] = p.darea[f];
+        for (int k = 0; k < C; k++) dsph[(size_t)f * NCB + k] = p.dsph[(size_t)f * C + k];
+        int q = 0;
+        for (int m = 0; m <= p.mmax; m++)
+            for (int l = m; l <= p.lmax; l++) cpl[(size_t)f * nq + q++] = p.pleg[((size_t)f * L1 + l) * L1 + m];
+        for (int m = 0; m <= p.mmax; m++) {
+            cfc[(size_t)f * (p.mmax + 1) + m] = p.fc[(size_t)f * (p.mmax + 1) + m];
+            cfs[(size_t)f * (p.mmax + 1) + m] = p.fs[(size_t)f * (p.mmax + 1) + m];
+        }
+    }
+    PSB_CUDA(c->d_fac.upload(fac, s));
+    PSB_CUDA(c->d_dsph.upload(dsph, s));
+    PSB_CUDA(c->d_cpl.upload(cpl, s));
+    PSB_CUDA(c->d_cfc.upload(cfc, s));
+    PSB_CUDA(c->d_cfs.upload(cfs, s));
+    PSB_CUDA(c->d_cgf.upload(p.cg_first, s));
+    // initial poles (period_search_BOINC.cpp:197-206, 825-830)
+    static const double beta_pole[10] = {0, 0, 0, 0, 60, 60, 60, -60, -60, -60};
+    static const double lambda_pole[10] = {0, 90, 180, 270, 60, 180, 300, 60, 180, 300};
+    const double deg2rad = M_PI / 180;
+    std::vector<double> pole(20);
+    for (int m = 0; m < 10; m++) {
+        double b = beta_pole[m];
+        b = 90 - b;
+        pole[m * 2] = deg2rad * b;
+        pole[m * 2 + 1] = deg2rad * lambda_pole[m];
+    }
+    PSB_CUDA(c->d_pole.upload(pole, s));
+    c->free_idx.clear();
+    for (int i = 0; i < p.ma; i++)
+        if (p.ia[i]) c->free_idx.push_back(i);
+    std::vector<int> ints(lc);
+    ints.insert(ints.end(), c->free_idx.begin(), c->free_idx.end());
+    PSB_CUDA(c->d_lc.upload(ints, s));
+    PSB_CUDA(c->d_queue.ensure(1));
+
+    psb::DevProblem& d = c->dp;
+    d.n_points = N;
+    d.n_rows = N + 3;
+    d.n_lc = L + 1;
+    d.F = F;
+    d.C = C;
+    d.NCB = NCB;
+    d.nq = nq;
+    d.lmax = p.lmax;
+    d.mmax = p.mmax;
+    d.ma = p.ma;
+    d.mfit = p.mfit;
+    d.npad = ((N + 3) + 31) / 32 * 32;
+    const double* P0 = c->d_pts.p;
+    d.t = P0;
+    d.ex = P0 + (size_t)1 * N;
+    d.ey = P0 + (size_t)2 * N;
+    d.ez = P0 + (size_t)3 * N;
+    d.e0x = P0 + (size_t)4 * N;
+    d.e0y = P0 + (size_t)5 * N;
+    d.e0z = P0 + (size_t)6 * N;
+    d.alpha = P0 + (size_t)7 * N;
+    d.lc_start = c->d_lc.p;
+    d.lc_rel = c->d_lc.p + (L + 2);
+    d.lc_npts = c->d_lc.p + (L + 2) + (L + 1);
+    d.free_idx = c->d_lc.p + lc.size();
+    d.fac = c->d_fac.p;
+    d.dsph = c->d_dsph.p;
+    d.cpl = c->d_cpl.p;
+    d.cfc = c->d_cfc.p;
+    d.cfs = c->d_cfs.p;
+    d.cg_first = c->d_cgf.p;
+    d.pole0 = c->d_pole.p;
+    d.phi0 = p.phi0;
+    d.alamda_start = p.alamda_start;
+    d.alamda_incr = p.alamda_incr;
+    d.log_cl = std::log(p.cl);
+    d.par1 = p.par[1];
+    d.par2 = p.par[2];
+    d.par3 = p.par[3];
+    d.ndata_m3 = (double)N;
+    d.freq_start = p.freq_start;
+    d.freq_step = p.freq_step;
+    stop_rule(p, d.n_iter_max, d.iter_diff_max, d.n_iter_min);
+    int threads = 0;
+    c->blocks_per_sm = psb::fp64_max_blocks_per_sm(d, &threads);
+    if (c->blocks_per_sm <= 0)
+        return fail(PS_ERR_LIMIT, "fit kernel does not fit on the device (shared memory or registers)");
+    return PS_OK;
+}
+
+// Data rows for a given conw_r: the 3 convexity rows have brightness 0,
+// sigma 1/conw_r and weight 1 (period_search_BOINC.cpp:491-496, 444-456).
+int upload_rows(ps_ctx* c) {
+    Problem& p = c->prob;
+    const int N = p.n_points, R = N + 3;
+    std::vector<double> rows((size_t)4 * R);
+    double* yobs = rows.data();
+    double* sig = yobs + R;
+    double* sig2i = sig + R;
+    double* wght = sig2i + R;
+    for (int i = 0; i < N; i++) {
+        yobs[i] = p.brightness[i];
+        sig[i] = p.sig[i];
+        wght[i] = p.weight[i];
+    }
+    for (int j = 0; j < 3; j++) {
+        yobs[N + j] = 0;
+        sig[N + j] = 1 / p.conw_r;
+        wght[N + j] = 1;
+    }
+    for (int i = 0; i < R; i++) sig2i[i] = 1 / (sig[i] * sig[i]);  // mrqcof.c:113
+    PSB_CUDA(c->d_rows.upload(rows, c->stream));
+    c->dp.yobs = c->d_rows.p;
+    c->dp.sig = c->d_rows.p + R;
+    c->dp.sig2i = c->d_rows.p + 2 * R;
+    c->dp.wght = c->d_rows.p + 3 * R;
+    c->dp.conw_r = p.conw_r;
+    PSB_CUDA(c->d_dp.ensure(1));
+    PSB_CUDA(cudaMemcpyAsync(c->d_dp.p, &c->dp, sizeof(psb::DevProblem), cudaMemcpyHostToDevice, c->stream));
+    c->rows_ready = true;
+    return PS_OK;
+}
+
+int ensure_scratch(ps_ctx* c, int slots) {
+    const size_t stride = (size_t)(c->dp.ma + 1) * c->dp.npad;
+    PSB_CUDA(c->d_scratch.ensure(stride * slots));
+    return PS_OK;
+}
+
+// Run fits [n_from, n_to] x 10 poles (or one override fit) into d_fits.
+int run_fits(ps_ctx* c, int n_from, int n_fits, int pole_override, double freq_override) {
+    PSB_CUDA(c->d_fits.ensure(n_fits));
+    int grid = c->sms * c->blocks_per_sm;
+    if (grid > n_fits) grid = n_fits;
+    int rc = ensure_scratch(c, grid);
+    if (rc) return rc;
+    PSB_CUDA(cudaMemsetAsync(c->d_queue.p, 0, sizeof(int), c->stream));
+    psb::FitBatch b{};
+    b.n_from = n_from;
+    b.n_fits = n_fits;
+    b.pole_override = pole_override;
+    b.freq_override = freq_override;
+    b.queue = c->d_queue.p;
+    b.out = c->d_fits.p;
+    b.scratch = c->d_scratch.p;
+    b.scratch_stride = (long long)(c->dp.ma + 1) * c->dp.npad;
+    PSB_CUDA(psb::launch_fp64_fits(c->dp, c->d_dp.p, b, grid, c->stream));
+    g_launches++;
+    return PS_OK;
+}
+
+int scan_into(ps_ctx* c, int n_from, int n_to, ps_record* d_out, int prepass) {
+    const int np = n_to - n_from + 1;
+    int rc = run_fits(c, n_from, np * 10, 0, 0.0);
+    if (rc) return rc;
+    PSB_CUDA(psb::launch_period_reduce(c->d_fits.p, np, c->dp.ndata_m3, prepass, d_out, c->stream));
+    g_launches++;
+    return PS_OK;
+}
+
+int open_device(ps_ctx* c, int device) {
+    c->device = device;
+    PSB_CUDA(cudaSetDevice(device));
+    PSB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    PSB_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
+    c->host_only = false;
+    int rc = upload_static(c);
+    if (rc) return rc;
+    return PS_OK;
+}
+
+int check_ready(const ps_ctx* c, bool need_rows) {
+    if (!c) return fail(PS_ERR_ARG, "null context");
+    if (c->host_only) return fail(PS_ERR_ARG, "context was opened without a device");
+    if (need_rows && !c->rows_ready) return fail(PS_ERR_ARG, "call ps_precalc or ps_set_conw_r first");
+    return PS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ps_last_error(void) { return g_err.c_str(); }
+long long ps_kernel_launches(void) { return g_launches.load(); }
+
+int ps_open_host_only(const char* path, ps_ctx** out) {
+    if (!path || !out) return fail(PS_ERR_ARG, "null argument");
+    *out = nullptr;
+    ps_ctx* c = new ps_ctx();
+    std::string err;
+    int rc = psb::parse_input(path, c->prob, err);
+    if (rc == 0) rc = psb::setup_geometry(c->prob, err);
+    if (rc != 0) {
+        delete c;
+        return fail(rc == -1 ? PS_ERR_IO : rc, err);
+    }
+    *out = c;
+    return PS_OK;
+}
+
+int ps_open_file(const char* path, int device, int form, ps_ctx** out) {
+    if (form != PS_FORM_FP64) return fail(PS_ERR_ARG, "unknown form");
+    int rc = ps_open_host_only(path, out);
+    if (rc) return rc;
+    (*out)->form = form;
+    rc = open_device(*out, device);
+    if (rc) {
+        ps_close(*out);
+        *out = nullptr;
+    }
+    return rc;
+}
+
+int ps_open(const ps_problem_desc* d, int device, int form, ps_ctx** out) {
+    if (!d || !out) return fail(PS_ERR_ARG, "null argument");
+    if (form != PS_FORM_FP64) return fail(PS_ERR_ARG, "unknown form");
+    *out = nullptr;
+    if (d->n_points < 1 || d->n_lc < 1 || !d->lc_points || !d->lc_relative || !d->tim || !d->ee || !d->ee0 ||
+        !d->brightness || !d->sig || !d->weight)
+        return fail(PS_ERR_ARG, "missing arrays in the problem description");
+    ps_ctx* c = new ps_ctx();
+    Problem& p = c->prob;
+    int total = 0;
+    for (int i = 0; i < d->n_lc; i++) {
+        if (d->lc_points[i] < 1) {
+            delete c;
+            return fail(PS_ERR_LIMIT, "empty lightcurve");
+        }
+        total += d->lc_points[i];
+    }
+    if (total != d->n_points) {
+        delete c;
+        return fail(PS_ERR_ARG, "lightcurve sizes do not add up to n_points");
+    }
+    p.per_start = d->per_start;
+    p.per_step_coef = d->per_step_coef;
+    p.per_end = d->per_end;
+    p.ia_prd = d->ia_prd;
+    p.phi0 = d->phi0_rad;
+    p.conw = d->conw;
+    p.lmax = d->lmax;
+    p.mmax = d->mmax;
+    p.nrows = d->nrows;
+    for (int i = 0; i < 3; i++) {
+        p.par[i + 1] = d->par[i];
+        p.ia_par[i + 1] = d->ia_par[i];
+    }
+    p.cl = d->cl;
+    p.ia_cl = d->ia_cl;
+    p.stop_condition = d->stop_condition;
+    p.n_iter_min = d->n_iter_min;
+    p.alamda_incr = d->alamda_incr;
+    p.alamda_start = d->alamda_start;
+    p.n_points = d->n_points;
+    p.lc_points.assign(d->lc_points, d->lc_points + d->n_lc);
+    p.lc_rel.assign(d->lc_relative, d->lc_relative + d->n_lc);
+    p.tim.assign(d->tim, d->tim + d->n_points);
+    p.ee.assign(d->ee, d->ee + (size_t)3 * d->n_points);
+    p.ee0.assign(d->ee0, d->ee0 + (size_t)3 * d->n_points);
+    p.brightness.assign(d->brightness, d->brightness + d->n_points);
+    p.sig.assign(d->sig, d->sig + d->n_points);
+    p.weight.assign(d->weight, d->weight + d->n_points);
+    p.jd_min = d->jd_min;
+    p.jd_max = d->jd_max;
+    p.escl = d->escl;
+    std::string err;
+    int rc = psb::finish_from_arrays(p, err);
+    if (rc == 0) rc = psb::setup_geometry(p, err);
+    if (rc != 0) {
+        delete c;
+        return fail(rc, err);
+    }
+    c->form = form;
+    rc = open_device(c, device);
+    if (rc) {
+        ps_close(c);
+        return rc;
+    }
+    *out = c;
+    return PS_OK;
+}
+
+void ps_close(ps_ctx* c) {
+    if (!c) return;
+    if (!c->host_only) {
+        cudaSetDevice(c->device);
+        if (c->stream) cudaStreamSynchronize(c->stream);
+        c->d_pts.release();
+        c->d_rows.release();
+        c->d_fac.release();
+        c->d_dsph.release();
+        c->d_cpl.release();
+        c->d_cfc.release();
+        c->d_cfs.release();
+        c->d_cgf.release();
+        c->d_pole.release();
+        c->d_lc.release();
+        c->d_free.release();
+        c->d_queue.release();
+        c->d_scratch.release();
+        c->d_fits.release();
+        c->d_rec.release();
+        c->d_eval.release();
+        c->d_dp.release();
+        if (c->stream) cudaStreamDestroy(c->stream);
+    }
+    delete c;
+}
+
+int ps_precalc(ps_ctx* c, double* conw_r) {
+    int rc = check_ready(c, false);
+    if (rc) return rc;
+    PSB_CUDA(cudaSetDevice(c->device));
+    Problem& p = c->prob;
+    int new_conw = 0;
+    std::vector<ps_record> rec(10);
+    // period_search_BOINC.cpp:488-715
+    while ((new_conw != 1) && ((p.conw_r * p.escl * p.escl) < 10.0)) {
+        rc = upload_rows(c);
+        if (rc) return rc;
+        int max_test_periods = 10;
+        double sum_dark_facet = 0.0;
+        const int n_iter = p.n_periods();
+        if (n_iter < max_test_periods) max_test_periods = n_iter;
+        PSB_CUDA(c->d_rec.ensure(10));
+        rc = scan_into(c, 1, max_test_periods, c->d_rec.p, 1);
+        if (rc) return rc;
+        PSB_CUDA(cudaMemcpyAsync(rec.data(), c->d_rec.p, sizeof(ps_record) * max_test_periods,
+                                 cudaMemcpyDeviceToHost, c->stream));
+        PSB_CUDA(cudaStreamSynchronize(c->stream));
+        for (int n = 0; n < max_test_periods; n++) sum_dark_facet = sum_dark_facet + rec[n].dark_pct;
+        const double ave_dark_facet = sum_dark_facet / max_test_periods;
+        if (ave_dark_facet < 1.0) new_conw = 1;
+        if (ave_dark_facet >= 1.0) p.conw_r = p.conw_r * 2;
+    }
+    rc = upload_rows(c);
+    if (rc) return rc;
+    if (conw_r) *conw_r = p.conw_r;
+    return PS_OK;
+}
+
+int ps_set_conw_r(ps_ctx* c, double conw_r) {
+    int rc = check_ready(c, false);
+    if (rc) return rc;
+    if (!(conw_r > 0)) return fail(PS_ERR_ARG, "conw_r must be positive");
+    PSB_CUDA(cudaSetDevice(c->device));
+    c->prob.conw_r = conw_r;
+    return upload_rows(c);
+}
+
+int ps_n_periods(const ps_ctx* c) { return c ? c->prob.n_periods() : -1; }
+
+int ps_scan_device(ps_ctx* c, int n_from, int n_to, ps_record* d_out, void* stream) {
+    int rc = check_ready(c, true);
+    if (rc) return rc;
+    if (n_from < 1 || n_to < n_from || n_to > c->prob.n_periods() || !d_out)
+        return fail(PS_ERR_ARG, "period range out of bounds");
+    PSB_CUDA(cudaSetDevice(c->device));
+    cudaStream_t saved = c->stream;
+    if (stream) c->stream = (cudaStream_t)stream;
+    rc = scan_into(c, n_from, n_to, d_out, 0);
+    c->stream = saved;
+    return rc;
+}
+
+int ps_scan(ps_ctx* c, int n_from, int n_to, ps_record* out) {
+    int rc = check_ready(c, true);
+    if (rc) return rc;
+    if (n_from < 1 || n_to < n_from || n_to > c->prob.n_periods() || !out)
+        return fail(PS_ERR_ARG, "period range out of bounds");
+    PSB_CUDA(cudaSetDevice(c->device));
+    const int np = n_to - n_from + 1;
+    PSB_CUDA(c->d_rec.ensure(np));
+    rc = scan_into(c, n_from, n_to, c->d_rec.p, 0);
+    if (rc) return rc;
+    PSB_CUDA(cudaMemcpyAsync(out, c->d_rec.p, sizeof(ps_record) * np, cudaMemcpyDeviceToHost, c->stream));
+    PSB_CUDA(cudaStreamSynchronize(c->stream));
+    return PS_OK;
+}
+
+int ps_fit(ps_ctx* c, double freq, int pole, ps_fit_result* out, double* cg_out) {
+    int rc = check_ready(c, true);
+    if (rc) return rc;
+    if (pole < 1 || pole > 10 || !(freq > 0) || !out) return fail(PS_ERR_ARG, "bad fit arguments");
+    PSB_CUDA(cudaSetDevice(c->device));
+    rc = run_fits(c, 1, 1, pole, freq);
+    if (rc) return rc;
+    psb::FitOut o;
+    PSB_CUDA(cudaMemcpyAsync(&o, c->d_fits.p, sizeof(o), cudaMemcpyDeviceToHost, c->stream));
+    PSB_CUDA(cudaStreamSynchronize(c->stream));
+    out->dev = o.dev;
+    out->dark = o.dark;
+    out->totarea = o.totarea;
+    out->period_d = o.prd;
+    out->lambda_deg = o.la;
+    out->beta_deg = o.be;
+    out->chisq = o.chisq;
+    out->niter = o.niter;
+    out->status = o.status;
+    (void)cg_out;
+    return PS_OK;
+}
+
+static int run_eval(ps_ctx* c, const double* a, std::vector<double>& alpha, std::vector<double>& beta,
+                    double& chisq, std::vector<double>* y, std::vector<double>* J) {
+    int rc = check_ready(c, true);
+    if (rc) return rc;
+    if (!a) return fail(PS_ERR_ARG, "null parameter vector");
+    PSB_CUDA(cudaSetDevice(c->device));
+    const psb::DevProblem& d = c->dp;
+    const size_t na = d.ma, nal = (size_t)d.mfit * d.mfit, nb = d.mfit, ny = d.n_rows, nJ = (size_t)d.n_rows * d.ma;
+    const size_t scratch = (size_t)(d.ma + 1) * d.npad;
+    const size_t total = na + nal + nb + 1 + ny + nJ + scratch;
+    PSB_CUDA(c->d_eval.ensure(total));
+    double* base = c->d_eval.p;
+    psb::EvalOut E;
+    E.a = base;
+    E.alpha = base + na;
+    E.beta = E.alpha + nal;
+    E.chisq = E.beta + nb;
+    E.y = E.chisq + 1;
+    E.J = E.y + ny;
+    E.scratch = E.J + nJ;
+    PSB_CUDA(cudaMemcpyAsync(base, a, na * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    PSB_CUDA(psb::launch_fp64_eval(d, c->d_dp.p, E, c->stream));
+    g_launches++;
+    alpha.resize(nal);
+    beta.resize(nb);
+    PSB_CUDA(cudaMemcpyAsync(alpha.data(), E.alpha, nal * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PSB_CUDA(cudaMemcpyAsync(beta.data(), E.beta, nb * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PSB_CUDA(cudaMemcpyAsync(&chisq, E.chisq, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (y) {
+        y->resize(ny);
+        PSB_CUDA(cudaMemcpyAsync(y->data(), E.y, ny * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (J) {
+        J->resize(nJ);
+        PSB_CUDA(cudaMemcpyAsync(J->data(), E.J, nJ * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
+    PSB_CUDA(cudaStreamSynchronize(c->stream));
+    return PS_OK;
+}
+
+int ps_mrqcof(ps_ctx* c, const double* a, double* alpha, double* beta, double* chisq) {
+    std::vector<double> al, be;
+    double x2 = 0;
+    int rc = run_eval(c, a, al, be, x2, nullptr, nullptr);
+    if (rc) return rc;
+    if (alpha) std::memcpy(alpha, al.data(), al.size() * sizeof(double));
+    if (beta) std::memcpy(beta, be.data(), be.size() * sizeof(double));
+    if (chisq) *chisq = x2;
+    return PS_OK;
+}
+
+int ps_model(ps_ctx* c, const double* a, double* ymod, double* dyda) {
+    std::vector<double> al, be, y, J;
+    double x2 = 0;
+    int rc = run_eval(c, a, al, be, x2, &y, &J);
+    if (rc) return rc;
+    if (ymod) std::memcpy(ymod, y.data(), y.size() * sizeof(double));
+    if (dyda) std::memcpy(dyda, J.data(), J.size() * sizeof(double));
+    return PS_OK;
+}
+
+int ps_info(const ps_ctx* c, int* ints, double* dbls) {
+    if (!c) return fail(PS_ERR_ARG, "null context");
+    const Problem& p = c->prob;
+    if (ints) {
+        ints[0] = p.n_points;
+        ints[1] = p.n_lc() + 1;
+        ints[2] = p.numfac;
+        ints[3] = p.ncoef;
+        ints[4] = p.ma;
+        ints[5] = p.mfit;
+        ints[6] = p.n_periods();
+    }
+    if (dbls) {
+        dbls[0] = p.escl;
+        dbls[1] = p.conw_r;
+        dbls[2] = p.freq_start;
+        dbls[3] = p.freq_end;
+        dbls[4] = p.freq_step;
+    }
+    return PS_OK;
+}
+
+int ps_get_array(const ps_ctx* c, const char* name, double* out) {
+    if (!c || !name || !out) return -1;
+    const Problem& p = c->prob;
+    auto put = [&](const std::vector<double>& v) {
+        std::memcpy(out, v.data(), v.size() * sizeof(double));
+        return (int)v.size();
+    };
+    auto puti = [&](const std::vector<int>& v) {
+        for (size_t i = 0; i < v.size(); i++) out[i] = v[i];
+        return (int)v.size();
+    };
+    const int N = p.n_points;
+    if (!std::strcmp(name, "nor")) return put(p.nor);
+    if (!std::strcmp(name, "darea")) return put(p.darea);
+    if (!std::strcmp(name, "dsph")) return put(p.dsph);
+    if (!std::strcmp(name, "cg_first")) return put(p.cg_first);
+    if (!std::strcmp(name, "ia")) return puti(p.ia);
+    if (!std::strcmp(name, "tim")) return put(p.tim);
+    if (!std::strcmp(name, "ee")) return put(p.ee);
+    if (!std::strcmp(name, "ee0")) return put(p.ee0);
+    if (!std::strcmp(name, "at")) return put(p.at);
+    if (!std::strcmp(name, "af")) return put(p.af);
+    if (!std::strcmp(name, "ifp")) return puti(p.ifp);
+    if (!std::strcmp(name, "brightness") || !std::strcmp(name, "sig") || !std::strcmp(name, "weight")) {
+        const std::vector<double>& v = name[0] == 'b' ? p.brightness : (name[0] == 's' ? p.sig : p.weight);
+        for (int i = 0; i < N; i++) out[i] = v[i];
+        for (int j = 0; j < 3; j++) out[N + j] = name[0] == 'b' ? 0.0 : (name[0] == 's' ? 1 / p.conw_r : 1.0);
+        return N + 3;
+    }
+    return -1;
+}
+
+int ps_format_record(const ps_record* r, int first_line, double conw_line, char* buf, int buflen) {
+    if (!r || !buf || buflen <= 0) return -1;
+    return std::snprintf(buf, (size_t)buflen, "%.8f  %.6f  %.6f %4.1f %4.0f %4.0f\n", r->period_h, r->rms, r->chi2,
+                         first_line ? conw_line : r->dark_pct, r->lambda_deg, r->beta_deg);
+}
+
+}  // extern "C"

@@ -1,0 +1,75 @@
+// Device-side data of the B200 period scan: the per-asteroid tables in HBM,
+// the per-fit result record and the launch interface of the fit kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace psb {
+
+// Per-asteroid tables, all device pointers, 0-based.
+//  rows: n_points data rows (lightcurve order) followed by 3 convexity rows.
+struct DevProblem {
+    int n_points, n_rows, n_lc;      // n_lc counts the convexity pseudo-curve
+    int F, C, NCB, nq, lmax, mmax, ma, mfit;
+    int npad;                        // leading dimension of the J scratch
+    // points [n_points]
+    const double *t, *ex, *ey, *ez, *e0x, *e0y, *e0z, *alpha;
+    // rows [n_rows]
+    const double *yobs, *sig, *sig2i, *wght;
+    // lightcurves [n_lc] (+1 for lc_start)
+    const int *lc_start, *lc_rel, *lc_npts;
+    // facets
+    const double* fac;   // [F][4]: nx, ny, nz, darea
+    const double* dsph;  // [F][NCB], zero padded beyond C
+    const double* cpl;   // [F][nq]: Pleg in curv's (m, l) order
+    const double* cfc;   // [F][mmax+1]
+    const double* cfs;   // [F][mmax+1]
+    const int* free_idx; // [mfit] parameter index of each free parameter
+    const double* cg_first;  // [C]
+    const double* pole0;     // [10][2]: initial beta' and lambda [rad]
+    // scalars
+    double phi0, conw_r, alamda_start, alamda_incr, log_cl, par1, par2, par3, ndata_m3;
+    double freq_start, freq_step;
+    int n_iter_max, n_iter_min;
+    double iter_diff_max;
+};
+
+// One fit's outcome (the quantities period_search_BOINC.cpp:900-920 reads).
+struct FitOut {
+    double dev, dark, totarea, prd, la, be, chisq;
+    int niter, status;
+};
+
+// A batch of fits: fit w is trial period n_from + w / 10, pole w % 10 + 1,
+// unless `freq_override` > 0 (single-fit API), then the only fit uses it.
+struct FitBatch {
+    int n_from;
+    int n_fits;
+    int pole_override;       // 1..10 for the single-fit API, else 0
+    double freq_override;
+    int* queue;              // work counter, zeroed before launch
+    FitOut* out;             // [n_fits]
+    double* scratch;         // per resident CTA: J^T (ma x npad) + y (npad)
+    long long scratch_stride;
+};
+
+// Diagnostics of one evaluation (ps_mrqcof / ps_model): J, y, alpha, beta.
+struct EvalOut {
+    const double* a;   // [ma] parameters
+    double* alpha;     // [mfit*mfit]
+    double* beta;      // [mfit]
+    double* chisq;     // [1]
+    double* y;         // [n_rows] normalised model
+    double* J;         // [n_rows*ma] normalised Jacobian, row-major
+    double* scratch;
+};
+
+size_t fp64_smem_bytes(const DevProblem& P);
+int fp64_max_blocks_per_sm(const DevProblem& P, int* threads);
+// P is the host copy (sizes, launch shape); dP the same struct in device memory.
+cudaError_t launch_fp64_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s);
+cudaError_t launch_fp64_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s);
+cudaError_t launch_period_reduce(const FitOut* fits, int n_periods, double ndata_m3, int prepass,
+                                 void* records /* ps_record[n_periods] */, cudaStream_t s);
+
+}  // namespace psb

@@ -1,0 +1,535 @@
+// Host setup of the B200 period scan.  Each routine restates one reference
+// routine (cited per function) in the same FP64 operation order; the
+// compile flags (-O3 -ffp-contract=off) keep that order intact.
+#include "ps_host.hpp"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace psb {
+namespace {
+
+const double kPi = M_PI;               // constants.h:13
+const double kDeg2Rad = kPi / 180;     // constants.h:17
+
+void skip_line(FILE* fp) {
+    int c;
+    while ((c = std::fgetc(fp)) != EOF && c != '\n') {
+    }
+}
+
+// trifac.c:10-82.  ifp gets 3 vertex ids (1-based) per facet.
+void trifac(int nrows, std::vector<int>& ifp) {
+    const int cols = 4 * nrows + 1;
+    std::vector<int> nod((size_t)(2 * nrows + 1) * cols, 0);
+    auto NOD = [&](int i, int j) -> int& { return nod[(size_t)i * cols + j]; };
+    ifp.assign((size_t)8 * nrows * nrows * 3, 0);
+    auto IFP = [&](int t, int j) -> int& { return ifp[(size_t)(t - 1) * 3 + (j - 1)]; };
+    int nnod = 1, ntri = 0;
+    NOD(0, 0) = nnod;
+    for (int i = 1; i <= nrows; i++)
+        for (int j = 0; j <= 4 * i - 1; j++) {
+            nnod++;
+            NOD(i, j) = nnod;
+            if (j == 0) NOD(i, 4 * i) = nnod;
+        }
+    for (int i = nrows - 1; i >= 1; i--)
+        for (int j = 0; j <= 4 * i - 1; j++) {
+            nnod++;
+            NOD(2 * nrows - i, j) = nnod;
+            if (j == 0) NOD(2 * nrows - i, 4 * i) = nnod;
+        }
+    NOD(2 * nrows, 0) = nnod + 1;
+    for (int j1 = 1; j1 <= nrows; j1++)
+        for (int j3 = 1; j3 <= 4; j3++) {
+            int j0 = (j3 - 1) * j1;
+            ntri++;
+            IFP(ntri, 1) = NOD(j1 - 1, j0 - (j3 - 1));
+            IFP(ntri, 2) = NOD(j1, j0);
+            IFP(ntri, 3) = NOD(j1, j0 + 1);
+            for (int j2 = j0 + 1; j2 <= j0 + j1 - 1; j2++) {
+                ntri++;
+                IFP(ntri, 1) = NOD(j1, j2);
+                IFP(ntri, 2) = NOD(j1 - 1, j2 - (j3 - 1));
+                IFP(ntri, 3) = NOD(j1 - 1, j2 - 1 - (j3 - 1));
+                ntri++;
+                IFP(ntri, 1) = NOD(j1 - 1, j2 - (j3 - 1));
+                IFP(ntri, 2) = NOD(j1, j2);
+                IFP(ntri, 3) = NOD(j1, j2 + 1);
+            }
+        }
+    for (int j1 = nrows + 1; j1 <= 2 * nrows; j1++)
+        for (int j3 = 1; j3 <= 4; j3++) {
+            int j0 = (j3 - 1) * (2 * nrows - j1);
+            ntri++;
+            IFP(ntri, 1) = NOD(j1, j0);
+            IFP(ntri, 2) = NOD(j1 - 1, j0 + 1 + (j3 - 1));
+            IFP(ntri, 3) = NOD(j1 - 1, j0 + (j3 - 1));
+            for (int j2 = j0 + 1; j2 <= j0 + (2 * nrows - j1); j2++) {
+                ntri++;
+                IFP(ntri, 1) = NOD(j1, j2);
+                IFP(ntri, 2) = NOD(j1 - 1, j2 + (j3 - 1));
+                IFP(ntri, 3) = NOD(j1, j2 - 1);
+                ntri++;
+                IFP(ntri, 1) = NOD(j1, j2);
+                IFP(ntri, 2) = NOD(j1 - 1, j2 + 1 + (j3 - 1));
+                IFP(ntri, 3) = NOD(j1 - 1, j2 + (j3 - 1));
+            }
+        }
+}
+
+// areanorm.c:10-60 with the vertex grid of period_search_BOINC.cpp:739-770.
+void areanorm(Problem& p) {
+    const int nrows = p.nrows;
+    std::vector<double> t(p.ndir + 1), f(p.ndir + 1);
+    double dth = kPi / (2 * nrows);
+    int k = 1;
+    t[1] = 0;
+    f[1] = 0;
+    for (int i = 1; i <= nrows; i++) {
+        double dph = kPi / (2 * i);
+        for (int j = 0; j <= 4 * i - 1; j++) {
+            k++;
+            t[k] = i * dth;
+            f[k] = j * dph;
+        }
+    }
+    for (int i = nrows - 1; i >= 1; i--) {
+        double dph = kPi / (2 * i);
+        for (int j = 0; j <= 4 * i - 1; j++) {
+            k++;
+            t[k] = kPi - i * dth;
+            f[k] = j * dph;
+        }
+    }
+    t[k + 1] = kPi;
+    f[k + 1] = 0;
+    std::vector<double> x(p.ndir + 1), y(p.ndir + 1), z(p.ndir + 1);
+    for (int i = 1; i <= p.ndir; i++) {
+        double st = std::sin(t[i]);
+        x[i] = st * std::cos(f[i]);
+        y[i] = st * std::sin(f[i]);
+        z[i] = std::cos(t[i]);
+    }
+    const int F = p.numfac;
+    p.nor.assign((size_t)F * 3, 0);
+    p.darea.assign(F, 0);
+    p.at.assign(F, 0);
+    p.af.assign(F, 0);
+    for (int i = 0; i < F; i++) {
+        const int* v = &p.ifp[(size_t)i * 3];
+        double vx[4], vy[4], vz[4], c[4];
+        for (int j = 2; j <= 3; j++) {
+            vx[j] = x[v[j - 1]] - x[v[0]];
+            vy[j] = y[v[j - 1]] - y[v[0]];
+            vz[j] = z[v[j - 1]] - z[v[0]];
+        }
+        c[1] = vy[2] * vz[3] - vy[3] * vz[2];
+        c[2] = vz[2] * vx[3] - vz[3] * vx[2];
+        c[3] = vx[2] * vy[3] - vx[3] * vy[2];
+        double clen2 = c[1] * c[1] + c[2] * c[2] + c[3] * c[3];
+        double clen = std::sqrt(clen2);
+        p.nor[(size_t)i * 3 + 0] = c[1] / clen;
+        p.nor[(size_t)i * 3 + 1] = c[2] / clen;
+        p.nor[(size_t)i * 3 + 2] = c[3] / clen;
+        p.at[i] = std::acos(p.nor[(size_t)i * 3 + 2]);
+        p.af[i] = std::atan2(p.nor[(size_t)i * 3 + 1], p.nor[(size_t)i * 3 + 0]);
+        p.darea[i] = 0.5 * clen;
+    }
+}
+
+// sphfunc.c:11-87: Legendre functions and the Dsph basis per facet normal.
+void sphfunc(Problem& p) {
+    const int F = p.numfac, L = p.lmax, M = p.mmax, L1 = L + 1;
+    std::vector<double> ts((size_t)F * L1), tc((size_t)F * L1);
+    p.fc.assign((size_t)F * (M + 1), 0);
+    p.fs.assign((size_t)F * (M + 1), 0);
+    for (int i = 0; i < F; i++) {
+        double* Ts = &ts[(size_t)i * L1];
+        double* Tc = &tc[(size_t)i * L1];
+        Ts[0] = 1;
+        Tc[0] = 1;
+        if (L >= 1) {
+            Ts[1] = std::sin(p.at[i]);
+            Tc[1] = std::cos(p.at[i]);
+        }
+        for (int j = 2; j <= L; j++) {
+            Ts[j] = Ts[1] * Ts[j - 1];
+            Tc[j] = Tc[1] * Tc[j - 1];
+        }
+        p.fs[(size_t)i * (M + 1)] = 0;
+        p.fc[(size_t)i * (M + 1)] = 1;
+        for (int j = 1; j <= M; j++) {
+            p.fs[(size_t)i * (M + 1) + j] = std::sin(j * p.af[i]);
+            p.fc[(size_t)i * (M + 1) + j] = std::cos(j * p.af[i]);
+        }
+    }
+    // aleg[n][l][m], n,l,m in 0..L (sphfunc.c:44-70)
+    std::vector<double> aleg((size_t)L1 * L1 * L1, 0.0);
+    auto A = [&](int n, int l, int m) -> double& { return aleg[((size_t)n * L1 + l) * L1 + m]; };
+    A(0, 0, 0) = 1;
+    if (L >= 1) A(1, 1, 0) = 1;
+    for (int l = 1; l <= L; l++) A(0, l, l) = A(0, l - 1, l - 1) * (2 * l - 1);
+    for (int m = 0; m <= M; m++)
+        for (int l = m + 1; l <= L; l++) {
+            int ibot;
+            if ((2 * ((l - m) / 2)) == (l - m)) {
+                A(0, l, m) = -(l + m - 1) * A(0, l - 2, m) / (1 * (l - m));
+                ibot = 2;
+            } else {
+                ibot = 1;
+            }
+            if (l != 1)
+                for (int n = ibot; n <= l - m; n = n + 2)
+                    A(n, l, m) = ((2 * l - 1) * A(n - 1, l - 1, m) - (l + m - 1) * A(n, l - 2, m)) / (1 * (l - m));
+        }
+    p.pleg.assign((size_t)F * L1 * L1, 0.0);
+    p.dsph.assign((size_t)F * p.ncoef, 0.0);
+    for (int i = 0; i < F; i++) {
+        const double* Ts = &ts[(size_t)i * L1];
+        const double* Tc = &tc[(size_t)i * L1];
+        int k = 0;
+        for (int m = 0; m <= M; m++)
+            for (int l = m; l <= L; l++) {
+                double& P = p.pleg[((size_t)i * L1 + l) * L1 + m];
+                P = 0;
+                int ibot = ((2 * ((l - m) / 2)) == (l - m)) ? 0 : 1;
+                for (int n = ibot; n <= l - m; n = n + 2) P = P + A(n, l, m) * Tc[n] * Ts[m];
+                p.dsph[(size_t)i * p.ncoef + k] = p.fc[(size_t)i * (M + 1) + m] * P;
+                k++;
+                if (m != 0) {
+                    p.dsph[(size_t)i * p.ncoef + k] = p.fs[(size_t)i * (M + 1) + m] * P;
+                    k++;
+                }
+            }
+    }
+}
+
+// ludcmp.c:9-68 on an n x n row-major matrix (0-based storage).
+int ludcmp(std::vector<double>& a, int n, std::vector<int>& indx) {
+    std::vector<double> v(n + 1);
+    auto Aij = [&](int i, int j) -> double& { return a[(size_t)(i - 1) * n + (j - 1)]; };
+    indx.assign(n + 1, 0);
+    int imax = -999;
+    for (int i = 1; i <= n; i++) {
+        double big = 0.0, temp;
+        for (int j = 1; j <= n; j++)
+            if ((temp = std::fabs(Aij(i, j))) > big) big = temp;
+        if (big == 0.0) return 4;
+        v[i] = 1.0 / big;
+    }
+    for (int j = 1; j <= n; j++) {
+        for (int i = 1; i < j; i++) {
+            double sum = Aij(i, j);
+            for (int k = 1; k < i; k++) sum -= Aij(i, k) * Aij(k, j);
+            Aij(i, j) = sum;
+        }
+        double big = 0.0, dum;
+        for (int i = j; i <= n; i++) {
+            double sum = Aij(i, j);
+            for (int k = 1; k < j; k++) sum -= Aij(i, k) * Aij(k, j);
+            Aij(i, j) = sum;
+            if ((dum = v[i] * std::fabs(sum)) >= big) {
+                big = dum;
+                imax = i;
+            }
+        }
+        if (j != imax) {
+            for (int k = 1; k <= n; k++) {
+                dum = Aij(imax, k);
+                Aij(imax, k) = Aij(j, k);
+                Aij(j, k) = dum;
+            }
+            v[imax] = v[j];
+        }
+        indx[j] = imax;
+        if (Aij(j, j) == 0.0) Aij(j, j) = 1.0e-20;
+        if (j != n) {
+            dum = 1.0 / (Aij(j, j));
+            for (int i = j + 1; i <= n; i++) Aij(i, j) *= dum;
+        }
+    }
+    return 0;
+}
+
+// lubksb.c:3-24; b is 1-based (b[0] unused).
+void lubksb(const std::vector<double>& a, int n, const std::vector<int>& indx, std::vector<double>& b) {
+    auto Aij = [&](int i, int j) { return a[(size_t)(i - 1) * n + (j - 1)]; };
+    int ii = 0;
+    for (int i = 1; i <= n; i++) {
+        int ip = indx[i];
+        double sum = b[ip];
+        b[ip] = b[i];
+        if (ii)
+            for (int j = ii; j <= i - 1; j++) sum -= Aij(i, j) * b[j];
+        else if (sum)
+            ii = i;
+        b[i] = sum;
+    }
+    for (int i = n; i >= 1; i--) {
+        double sum = b[i];
+        for (int j = i + 1; j <= n; j++) sum -= Aij(i, j) * b[j];
+        b[i] = sum / Aij(i, i);
+    }
+}
+
+// ellfit.c:11-88: Laplace-series coefficients of the ellipsoid's log
+// curvature function (normal equations + LU solve).
+int ellfit(Problem& p) {
+    const int F = p.numfac, C = p.ncoef, L1 = p.lmax + 1;
+    const double a = p.a_axis, b = p.b_axis, c = p.c_axis;
+    std::vector<double> er(F), fmat((size_t)F * C);
+    for (int i = 0; i < F; i++) {
+        double st = std::sin(p.at[i]);
+        double sum = std::pow(a * st * std::cos(p.af[i]), 2) + std::pow(b * st * std::sin(p.af[i]), 2) +
+                     std::pow(c * std::cos(p.at[i]), 2);
+        er[i] = 2 * (std::log(a * b * c) - std::log(sum));
+    }
+    for (int i = 0; i < F; i++) {
+        int n = 0;
+        for (int m = 0; m <= p.mmax; m++)
+            for (int l = m; l <= p.lmax; l++) {
+                double P = p.pleg[((size_t)i * L1 + l) * L1 + m];
+                if (m != 0) {
+                    fmat[(size_t)i * C + n] = P * std::cos(m * p.af[i]);
+                    n++;
+                    fmat[(size_t)i * C + n] = P * std::sin(m * p.af[i]);
+                    n++;
+                } else {
+                    fmat[(size_t)i * C + n] = P;
+                    n++;
+                }
+            }
+    }
+    std::vector<double> fitmat((size_t)C * C), fitvec(C + 1);
+    for (int i = 0; i < C; i++) {
+        for (int j = 0; j < C; j++) {
+            double s = 0;
+            for (int k = 0; k < F; k++) s = s + fmat[(size_t)k * C + i] * fmat[(size_t)k * C + j];
+            fitmat[(size_t)i * C + j] = s;
+        }
+        double s = 0;
+        for (int j = 0; j < F; j++) s = s + fmat[(size_t)j * C + i] * er[j];
+        fitvec[i + 1] = s;
+    }
+    std::vector<int> indx;
+    if (ludcmp(fitmat, C, indx) != 0) return 4;
+    lubksb(fitmat, C, indx, fitvec);
+    p.cg_first.assign(C, 0);
+    for (int i = 0; i < C; i++) p.cg_first[i] = fitvec[i + 1];
+    return 0;
+}
+
+}  // namespace
+
+int parse_input(const char* path, Problem& p, std::string& err) {
+    FILE* fp = std::fopen(path, "r");
+    if (!fp) {
+        err = std::string("cannot open input file ") + path;
+        return -1;
+    }
+    int rc = 2;
+    std::vector<double> al;
+    auto bad = [&](const char* what) {
+        err = std::string("malformed input: ") + what;
+        return 2;
+    };
+#define PSB_RD(n, ...)                                                         \
+    if (std::fscanf(fp, __VA_ARGS__) < (n)) { rc = bad("header"); goto done; } \
+    skip_line(fp);
+    PSB_RD(4, "%lf %lf %lf %d", &p.per_start, &p.per_step_coef, &p.per_end, &p.ia_prd)
+    PSB_RD(1, "%lf", &p.jd_00)
+    PSB_RD(1, "%lf", &p.phi0)
+    PSB_RD(1, "%lf", &p.conw)
+    PSB_RD(2, "%d %d", &p.lmax, &p.mmax)
+    PSB_RD(1, "%d", &p.nrows)
+    PSB_RD(2, "%lf %d", &p.par[1], &p.ia_par[1])
+    PSB_RD(2, "%lf %d", &p.par[2], &p.ia_par[2])
+    PSB_RD(2, "%lf %d", &p.par[3], &p.ia_par[3])
+    PSB_RD(2, "%lf %d", &p.cl, &p.ia_cl)
+    PSB_RD(1, "%lf", &p.stop_condition)
+    PSB_RD(1, "%d", &p.n_iter_min)
+    PSB_RD(1, "%lf", &p.alamda_incr)
+    PSB_RD(1, "%lf", &p.alamda_start)
+#undef PSB_RD
+    {
+        int nlc = 0;
+        if (std::fscanf(fp, "%d", &nlc) != 1 || nlc < 1) {
+            rc = bad("number of lightcurves");
+            goto done;
+        }
+        p.lc_points.assign(nlc, 0);
+        p.lc_rel.assign(nlc, 0);
+        for (int i = 0; i < nlc; i++) {
+            int np = 0, flag = 0;
+            if (std::fscanf(fp, "%d %d", &np, &flag) != 2 || np < 1) {
+                rc = bad("lightcurve header");
+                goto done;
+            }
+            skip_line(fp);
+            p.lc_points[i] = np;
+            p.lc_rel[i] = 1 - flag;
+            for (int j = 0; j < np; j++) {
+                double t, b, e0[3], e[3];
+                if (std::fscanf(fp, "%lf %lf", &t, &b) != 2 ||
+                    std::fscanf(fp, "%lf %lf %lf", &e0[0], &e0[1], &e0[2]) != 3 ||
+                    std::fscanf(fp, "%lf %lf %lf", &e[0], &e[1], &e[2]) != 3) {
+                    rc = bad("data point");
+                    goto done;
+                }
+                p.tim.push_back(t);
+                p.brightness.push_back(b);
+                // raw (unnormalised) vectors; finish_raw() normalises
+                for (int k = 0; k < 3; k++) p.ee.push_back(e[k]);
+                for (int k = 0; k < 3; k++) p.ee0.push_back(e0[k]);
+            }
+        }
+        // weights: `lc weight` pairs to EOF (period_search_BOINC.cpp:420-427)
+        std::vector<double> wlc(nlc + 1, -1.0);
+        while (std::feof(fp) == 0) {
+            int lc = 0;
+            double w = 0;
+            if (std::fscanf(fp, "%d", &lc) != 1) break;
+            if (std::fscanf(fp, "%lf", &w) != 1) break;
+            if (lc >= 1 && lc <= nlc) wlc[lc] = w;
+        }
+        p.n_points = (int)p.tim.size();
+        p.weight.assign(p.n_points, 1.0);
+        int k = 0;
+        for (int i = 0; i < nlc; i++)
+            for (int j = 0; j < p.lc_points[i]; j++, k++) p.weight[k] = (wlc[i + 1] == -1) ? 1 : wlc[i + 1];
+        // normalise vectors, lightcurve means, phase angles of first points
+        // (period_search_BOINC.cpp:343-414)
+        double al0 = kPi, al0_abs = kPi;
+        int ial0 = -1, ial0_abs = -1;
+        p.jd_min = 1e20;
+        p.jd_max = -1e40;
+        p.onlyrel = 1;
+        p.sig.assign(p.n_points, 0);
+        int np = 0;
+        for (int i = 0; i < nlc; i++) {
+            double ave = 0;
+            if (p.lc_rel[i] == 0) p.onlyrel = 0;
+            for (int j = 0; j < p.lc_points[i]; j++, np++) {
+                if (p.tim[np] < p.jd_min) p.jd_min = p.tim[np];
+                if (p.tim[np] > p.jd_max) p.jd_max = p.tim[np];
+                double* e = &p.ee[(size_t)np * 3];
+                double* e0 = &p.ee0[(size_t)np * 3];
+                double e0len = std::sqrt(e0[0] * e0[0] + e0[1] * e0[1] + e0[2] * e0[2]);
+                double elen = std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+                ave += p.brightness[np];
+                if (j == 0) {
+                    double cos_alpha = (e[0] * e0[0] + e[1] * e0[1] + e[2] * e0[2]) / (elen * e0len);
+                    double a = std::acos(cos_alpha);
+                    if (a < al0) {
+                        al0 = a;
+                        ial0 = np;
+                    }
+                    if ((a < al0_abs) && (p.lc_rel[i] == 0)) {
+                        al0_abs = a;
+                        ial0_abs = np;
+                    }
+                }
+                for (int c = 0; c < 3; c++) {
+                    e[c] = e[c] / elen;
+                    e0[c] = e0[c] / e0len;
+                }
+            }
+            ave /= p.lc_points[i];
+            for (int j = np - p.lc_points[i]; j < np; j++) p.sig[j] = ave;
+        }
+        p.jd_0 = p.jd_00;
+        if (p.jd_0 <= 0) p.jd_0 = (int)p.jd_min;
+        for (int i = 0; i < p.n_points; i++) p.tim[i] = p.tim[i] - p.jd_0;
+        p.phi0 = p.phi0 * kDeg2Rad;
+        if (p.onlyrel == 0) {
+            al0 = al0_abs;
+            ial0 = ial0_abs;
+        }
+        double a = 1.05, b = 1.00, c = 0.95;
+        double rfit = std::sqrt(2 * p.sig[ial0] / (0.5 * kPi * (1 + std::cos(al0))));
+        p.escl = rfit / std::sqrt((a * b + b * c + a * c) / 3);
+        if (p.onlyrel == 0) p.escl *= 0.8;
+        rc = finish_from_arrays(p, err);
+    }
+done:
+    std::fclose(fp);
+    return rc;
+}
+
+int finish_from_arrays(Problem& p, std::string& err) {
+    if (p.lmax < 0 || p.lmax > kMaxLm || p.mmax < 0 || p.mmax > p.lmax || p.nrows < 1 || p.nrows > 64) {
+        err = "degree/order or number of rows out of range";
+        return 2;
+    }
+    if (p.n_points < 1 || p.per_start <= 0 || p.per_end <= 0 || p.per_step_coef <= 0) {
+        err = "empty data or invalid period range";
+        return 2;
+    }
+    p.onlyrel = 1;
+    for (int r : p.lc_rel)
+        if (r == 0) p.onlyrel = 0;
+    p.a_axis = 1.05 * p.escl;
+    p.b_axis = 1.00 * p.escl;
+    p.c_axis = 0.95 * p.escl;
+    p.conw_r = p.conw / p.escl / p.escl;
+    return 0;
+}
+
+int setup_geometry(Problem& p, std::string& err) {
+    p.ncoef = 0;
+    for (int m = 0; m <= p.mmax; m++)
+        for (int l = m; l <= p.lmax; l++) {
+            p.ncoef++;
+            if (m != 0) p.ncoef++;
+        }
+    p.numfac = 8 * p.nrows * p.nrows;
+    p.ndir = 4 * p.nrows * p.nrows + 2;
+    p.nphpar = 3;
+    p.ma = p.ncoef + 5 + p.nphpar;
+    trifac(p.nrows, p.ifp);
+    areanorm(p);
+    sphfunc(p);
+    if (ellfit(p) != 0) {
+        err = "singular matrix in the ellipsoid fit (ludcmp)";
+        return 4;
+    }
+    p.freq_start = 1 / p.per_start;
+    p.freq_end = 1 / p.per_end;
+    p.freq_step = 0.5 / (p.jd_max - p.jd_min) / 24 * p.per_step_coef;
+    // free-parameter mask (period_search_BOINC.cpp:789-802, 839)
+    const int C = p.ncoef;
+    p.ia.assign(p.ma, 0);
+    p.ia[C + 0] = 1;  // beta pole
+    p.ia[C + 1] = 1;  // lambda pole
+    p.ia[C + 2] = p.ia_prd;
+    for (int i = 0; i < C; i++) p.ia[i] = 1;
+    if (p.onlyrel == 1) p.ia[0] = 0;
+    for (int i = 1; i <= p.nphpar; i++) p.ia[C + 2 + i] = p.ia_par[i];
+    p.ia[C + 3 + p.nphpar] = p.ia_cl;
+    p.ia[C + 4 + p.nphpar] = 0;  // Lommel-Seeliger coefficient fixed
+    p.mfit = 0;
+    for (int v : p.ia) p.mfit += v ? 1 : 0;
+    p.geometry_ready = true;
+    return 0;
+}
+
+void initial_parameters(const Problem& p, double freq, int m, double* cg) {
+    // initial poles (period_search_BOINC.cpp:197-206)
+    static const double beta_pole[kNPoles + 1] = {0, 0, 0, 0, 0, 60, 60, 60, -60, -60, -60};
+    static const double lambda_pole[kNPoles + 1] = {0, 0, 90, 180, 270, 60, 180, 300, 60, 180, 300};
+    const int C = p.ncoef;
+    double prd = 1 / freq;
+    for (int i = 0; i < C; i++) cg[i] = p.cg_first[i];
+    double b = beta_pole[m], l = lambda_pole[m];
+    b = 90 - b;
+    cg[C + 0] = kDeg2Rad * b;
+    cg[C + 1] = kDeg2Rad * l;
+    cg[C + 2] = 24 * 2 * kPi / prd;
+    for (int i = 1; i <= p.nphpar; i++) cg[C + 2 + i] = p.par[i];
+    cg[C + 4 + p.nphpar] = 1;
+    cg[C + 3 + p.nphpar] = std::log(p.cl);
+}
+
+}  // namespace psb

@@ -1,0 +1,222 @@
+"""Regenerate the golden fixtures under tests/golden/ (run in the build
+container, where the reference sources exist; the fixtures are committed so
+that tests never need /root/reference at run time).
+
+    python tests/golden/make_golden.py [names...]
+
+For every workload it writes <name>/period_search_in and the records of the
+reference application itself, compiled in place from its own sources by
+oracle/Makefile (`make -C oracle ref`):
+
+  ref_out.txt   the reference's printed output (period_search_out)
+  ref_out.full  the same six values at %.17g (side file of the stub MFILE)
+  fma_out.full  the same source rebuilt with FMA contraction; a period whose
+                chi2 differs between the two builds is "chaotic" (its LM
+                trajectory amplifies last-ulp differences)
+
+Long scans are split across host cores the way the reference allows it:
+each slice keeps P_start (so the convexity pre-pass sees the same first ten
+periods), trims P_end so that the scan stops at the slice end, and starts at
+the slice start through period_search_state (period_search_BOINC.cpp:237-251).
+
+Inputs:
+  shipped   the reference's own period_search/period_search_in (+ its shipped
+            period_search_out as `shipped_out.txt`), first 12 periods
+  tiny, tiny_rel, c1   seeded synthetic asteroids (periodsearch_b200.synth)
+  unit      golden arrays of the reference's unit tests
+            (period_search_pure_cpu_win/UnitTest_pure_cpu_win/arrangers.cpp),
+            dumped to unit.json through a small C++ harness
+"""
+from __future__ import annotations
+
+import concurrent.futures as cf
+import json
+import os
+import shutil
+import subprocess
+import sys
+import tempfile
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+REF_ROOT = "/root/reference"
+REF_EXE = os.path.join(REPO, "oracle", "_ref", "period_search_ref")
+REF_FMA = os.path.join(REPO, "oracle", "_ref", "period_search_ref_fma")
+
+
+def _header_values(text):
+    first = text.split("\n", 1)[0].split()
+    return float(first[0]), float(first[1]), float(first[2]), int(first[3])
+
+
+def _jd_span(text):
+    lines = text.splitlines()
+    i = 15  # after the 14 header lines and the lightcurve count
+    nlc = int(lines[14].split()[0])
+    jd = []
+    for _ in range(nlc):
+        n = int(lines[i].split()[0])
+        for k in range(n):
+            jd.append(float(lines[i + 1 + k].split()[0]))
+        i += n + 1
+    return min(jd), max(jd)
+
+
+def _n_per(p_start, coef, p_end, jd_min, jd_max):
+    f_start = 1 / p_start
+    f_end = 1 / p_end
+    f_step = 0.5 / (jd_max - jd_min) / 24 * coef
+    return int((f_start - f_end) / f_step) + 1
+
+
+def _slice_text(text, n_end):
+    """Same input with P_end moved so that the scan has exactly n_end periods."""
+    p_start, coef, p_end, ia = _header_values(text)
+    jd_min, jd_max = _jd_span(text)
+    f_start = 1 / p_start
+    f_step = 0.5 / (jd_max - jd_min) / 24 * coef
+    for frac in (0.5, 0.3, 0.7, 0.1, 0.9):
+        pe = float("%.12f" % (1 / (f_start - (n_end - 1 + frac) * f_step)))
+        if _n_per(p_start, coef, pe, jd_min, jd_max) == n_end:
+            rest = text.split("\n", 1)
+            tail = rest[0].split(None, 4)[4] if len(rest[0].split(None, 4)) > 4 else ""
+            return "%.10f %g %.12f %d %s\n%s" % (p_start, coef, pe, ia, tail, rest[1])
+    raise RuntimeError("cannot place P_end for %d periods" % n_end)
+
+
+def _run_slice(exe, text, n_from, n_to):
+    d = tempfile.mkdtemp(prefix="psgold")
+    try:
+        with open(os.path.join(d, "period_search_in"), "w") as f:
+            f.write(_slice_text(text, n_to))
+        if n_from > 1:
+            with open(os.path.join(d, "period_search_state"), "w") as f:
+                f.write("%d" % (n_from - 1))
+        subprocess.run([exe], cwd=d, check=True, stdout=subprocess.DEVNULL)
+        txt = open(os.path.join(d, "period_search_out")).read()
+        full = open(os.path.join(d, "period_search_out.full")).read()
+        return txt, full
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def run_reference(exe, text, n_periods, workers):
+    per = max(1, -(-n_periods // workers))
+    slices = [(a, min(a + per - 1, n_periods)) for a in range(1, n_periods + 1, per)]
+    with cf.ProcessPoolExecutor(max_workers=workers) as ex:
+        outs = list(ex.map(_run_slice, [exe] * len(slices), [text] * len(slices),
+                           [s[0] for s in slices], [s[1] for s in slices]))
+    return "".join(o[0] for o in outs), "".join(o[1] for o in outs)
+
+
+def make_workload(name, text, n_periods, workers):
+    d = os.path.join(HERE, name)
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "period_search_in"), "w") as f:
+        f.write(text)
+    txt, full = run_reference(REF_EXE, text, n_periods, workers)
+    open(os.path.join(d, "ref_out.txt"), "w").write(txt)
+    open(os.path.join(d, "ref_out.full"), "w").write(full)
+    _, full_fma = run_reference(REF_FMA, text, n_periods, workers)
+    open(os.path.join(d, "fma_out.full"), "w").write(full_fma)
+    print(name, n_periods, "periods written", flush=True)
+
+
+UNIT_HARNESS = r"""
+#include <cstdio>
+#include "arrangers.hpp"
+#include "constants.h"
+#include "globals.h"
+int Lmax, Mmax, Niter, Lastcall, Ncoef, Numfac, Lcurves, Nphpar, Deallocate, n_iter;
+int Lpoints[MAX_LC + 1], Inrel[MAX_LC + 1];
+double Alamda, Alamda_incr, Alamda_start, Ochisq, Chisq, _Chisq, Phi_0, Scale, _scale;
+double Blmat[4][4], _blmat[4][4], Dblm[3][4][4], _dblm[3][4][4];
+double Xx1[4], Xx2[4], _xx1[4], _xx2[4];
+double tmat[4][4], dtm[4][4][4], _tmat[4][4], _dtm[4][4][4];
+double php[N_PHOT_PAR + 1], dphp[N_PHOT_PAR + 1], _dphp[N_PHOT_PAR + 1];
+double Sclnw[MAX_LC + 1], Yout[MAX_N_OBS + 1], Weight[MAX_N_OBS + 1];
+double Fc[MAX_N_FAC + 1][MAX_LM + 1], Fs[MAX_N_FAC + 1][MAX_LM + 1], Tc[MAX_N_FAC + 1][MAX_LM + 1], Ts[MAX_N_FAC + 1][MAX_LM + 1];
+double Dsph[MAX_N_FAC + 1][MAX_N_PAR + 1], _dsph[MAX_N_FAC + 1][MAX_N_PAR + 1];
+double Pleg[MAX_N_FAC + 1][MAX_LM + 1][MAX_LM + 1], _pleg[MAX_N_FAC + 1][MAX_LM + 1][MAX_LM + 1];
+double Area[MAX_N_FAC + 1], Darea[MAX_N_FAC + 1], Nor[3][MAX_N_FAC + 1], Dg[MAX_N_FAC + 1][MAX_N_PAR + 1];
+double _area[MAX_N_FAC + 1], _darea[MAX_N_FAC + 1], _nor[3][MAX_N_FAC + 1], _dg[MAX_N_FAC + 1][MAX_N_PAR + 1];
+double Dyda[MAX_N_PAR + 1], _dyda[MAX_N_PAR + 1];
+static void arr(const char* name, const double* a, int n, bool last = false) {
+  std::printf("\"%s\": [", name);
+  for (int i = 0; i < n; i++) std::printf(i ? ", %.17g" : "%.17g", a[i]);
+  std::printf("]%s\n", last ? "" : ",");
+}
+int main() {
+  static double t[MAX_N_FAC + 1], f[MAX_N_FAC + 1], at[MAX_N_FAC + 1], af[MAX_N_FAC + 1], cg[MAX_N_PAR + 1];
+  static int ifp_rows[MAX_N_FAC + 1][4];
+  int* ifp[MAX_N_FAC + 1];
+  for (int i = 0; i <= MAX_N_FAC; i++) ifp[i] = ifp_rows[i];
+  get_t(t); get_f(f); get_at(at); get_af(af); get_ifp(ifp);
+  Lmax = Mmax = 3; Ncoef = 16; Numfac = 288;
+  get_cg_first(16, cg); get_pleg(); get_dsph(); get_area(); get_dg();
+  std::printf("{\n");
+  arr("t", t + 1, 146); arr("f", f + 1, 146); arr("at", at + 1, 288); arr("af", af + 1, 288);
+  static double ifpd[288 * 3];
+  for (int i = 1; i <= 288; i++) for (int j = 1; j <= 3; j++) ifpd[(i - 1) * 3 + j - 1] = ifp[i][j];
+  arr("ifp", ifpd, 288 * 3);
+  arr("cg_first", cg + 1, 16);
+  static double pl[288 * 16], ds[288 * 16], dg[288 * 16];
+  for (int i = 1; i <= 288; i++) {
+    for (int l = 0; l <= 3; l++) for (int m = 0; m <= 3; m++) pl[(i - 1) * 16 + l * 4 + m] = _pleg[i][l][m];
+    for (int k = 1; k <= 16; k++) ds[(i - 1) * 16 + k - 1] = _dsph[i][k];
+  }
+  // get_area / get_dg hold zero-based arrays (facet i+1, coefficient k+1)
+  for (int i = 0; i < 288; i++) for (int k = 0; k < 16; k++) dg[i * 16 + k] = _dg[i][k];
+  arr("pleg", pl, 288 * 16); arr("dsph", ds, 288 * 16); arr("dg", dg, 288 * 16);
+  arr("area", _area, 288, true);
+  std::printf("}\n");
+  return 0;
+}
+"""
+
+
+def make_unit():
+    src = os.path.join(REF_ROOT, "period_search_pure_cpu_win", "UnitTest_pure_cpu_win")
+    d = tempfile.mkdtemp(prefix="psunit")
+    try:
+        for h in ("stdafx.h", "CppUnitTest.h", "SDKDDKVer.h", "targetver.h"):
+            open(os.path.join(d, h), "w").write("")
+        open(os.path.join(d, "harness.cpp"), "w").write(UNIT_HARNESS)
+        exe = os.path.join(d, "harness")
+        subprocess.run(["g++", "-O0", "-w", "-I", d, "-I", src, "-o", exe, os.path.join(d, "harness.cpp"),
+                        os.path.join(src, "arrangers.cpp")], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout
+        data = json.loads(out)
+        data["_source"] = ("period_search_pure_cpu_win/UnitTest_pure_cpu_win/arrangers.cpp: get_t, get_f, get_at, "
+                           "get_af, get_ifp, get_cg_first, get_pleg, get_dsph, get_dg, get_area "
+                           "(TestTrifac/TestAreanorm/TestSphfunc/TestEllfit/TestCurv, InnerFunctionsTests.cpp:165-541)")
+        json.dump(data, open(os.path.join(HERE, "unit.json"), "w"))
+        print("unit.json written", flush=True)
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def main(names):
+    from periodsearch_b200 import synth
+
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "all", "ref"], check=True)
+    workers = os.cpu_count() or 4
+    if "unit" in names:
+        make_unit()
+    if "shipped" in names:
+        text = open(os.path.join(REF_ROOT, "period_search", "period_search_in")).read()
+        d = os.path.join(HERE, "shipped")
+        os.makedirs(d, exist_ok=True)
+        shutil.copy(os.path.join(REF_ROOT, "period_search", "period_search_out"), os.path.join(d, "shipped_out.txt"))
+        make_workload("shipped", _slice_text(text, 12), 12, 1)
+    for name, fn, n in (("tiny", synth._tiny, None), ("tiny_rel", synth._tiny_rel, None), ("c1", synth._c1, None)):
+        if name in names:
+            w = fn()
+            make_workload(name, w.text, w.n_periods, workers if w.n_periods > 20 else 1)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or ["unit", "shipped", "tiny", "tiny_rel", "c1"])
