@@ -92,7 +92,7 @@ class ClockSampler:
         sm = [float(r[1]) for r in rows]
         smax = float(rows[0][2])
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if "Active" in r[5 + i]})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows)}
 
 
@@ -164,7 +164,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--periods-per-step", type=int, default=592)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile", action="store_true",
+                    help="small case for ncu: 14 periods per step, no pre-pass, no e2e/cpu legs")
     args = ap.parse_args()
+    if args.profile:
+        args.periods_per_step = 14
+        args.no_cpu = args.no_e2e = True
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -197,13 +203,20 @@ def main():
     # convexity-weight pre-pass (100 fits per round), timed on its own
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    conw_r = g.precalc()
+    if args.profile:
+        conw_r = g.conw_r
+        g.set_conw_r(conw_r)
+    else:
+        conw_r = g.precalc()
     torch.cuda.synchronize()
     prepass_s = time.perf_counter() - t0
     n_total = g.n_periods
     B = args.periods_per_step
     fits_per_step = 10 * B
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the C ABI treats a NULL stream as "the library's own
+    # stream", and torch's default stream has handle 0
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     d_rec = torch.zeros(B * 6, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -238,11 +251,11 @@ def main():
     clocks = clk.summary()
 
     # e2e through the public API from host buffers
-    rec_host = None
+    rec_host = np.zeros(B, dtype=ps.RECORD_DTYPE)
     e2e_times = []
     desc = _desc_from(g, path)
     h2d = sum(np.asarray(v).nbytes for v in desc.values() if isinstance(v, np.ndarray))
-    for s in range(args.steps + 1):
+    for s in range(0 if args.no_e2e else min(args.steps, 3) + 1):
         a, b = batch(args.warmup + s)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -253,7 +266,7 @@ def main():
         dt = time.perf_counter() - t0
         if s:
             e2e_times.append(dt)
-    e2e_value = world * fits_per_step * len(e2e_times) / sum(e2e_times)
+    e2e_value = world * fits_per_step * len(e2e_times) / sum(e2e_times) if e2e_times else None
 
     # check a few records of the last timed batch against the same call again
     got = d_rec.view(B, 6).cpu().numpy()

@@ -76,7 +76,7 @@ struct pso_problem {
     /* LM state: the reference keeps these process-global (globals.h:5-6,
        mrqmin.c:17-19) and they carry from one fit to the next */
     double ochisq, chisq, alamda;
-    int niter;
+    int niter, lm_status;
     double *atry, *lm_beta, *da, *covar, *alpha, *cg;
 };
 
@@ -772,7 +772,10 @@ static int mrqmin(pso_problem* p, double* a) {
         p->da[j] = p->lm_beta[j];
     }
     err_code = gauss_errc1(p->covar, mfit, p->da);
-    if (err_code != 0) return err_code;
+    if (err_code != 0) {
+        if (p->lm_status == 0) p->lm_status = err_code;
+        return err_code;
+    }
     j = 0;
     for (l = 1; l <= ma; l++)
         if (p->ia[l]) {
@@ -1123,6 +1126,7 @@ static void run_fit(pso_problem* p, double freq, int m, double* out) {
     }
     p->alamda = -1;
     p->niter = 0;
+    p->lm_status = 0;
     iter_diff = 1e40;
     dev_old = 1e30;
     dev_new = 0;
@@ -1160,13 +1164,14 @@ static void run_fit(pso_problem* p, double freq, int m, double* out) {
     out[6] = p->chisq;
     out[7] = p->niter;
     out[8] = p->alamda;
+    out[9] = p->lm_status;
     (void)ma;
 }
 
 /* Best-of-poles record for trial period n (:811-924). */
 static void run_period(pso_problem* p, int n, int prepass, pso_record* rec) {
     double freq = p->freq_start - (n - 1) * p->freq_step;
-    double per_best = 0, dark_best = 0, la_best = 0, be_best = 0, dev_best = 1e40, out[9];
+    double per_best = 0, dark_best = 0, la_best = 0, be_best = 0, dev_best = 1e40, out[10];
     int m;
     for (m = 1; m <= PSO_N_POLES; m++) {
         run_fit(p, freq, m, out);

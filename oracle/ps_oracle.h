@@ -51,7 +51,8 @@ int pso_scan(pso_problem* p, int n_from, int n_to, pso_record* out);
 
 /* One LM fit at trial frequency freq [1/day] from initial pole m (1..10)
  * (period_search_BOINC.cpp:817-920).  out[0..8] = dev, dark (|chck|),
- * totarea, prd [day], lambda [deg], beta [deg], chisq, niter, alamda;
+ * totarea, prd [day], lambda [deg], beta [deg], chisq, niter, alamda, status
+ * (the first gauss_errc code of the fit, 0 if none; out has 10 slots);
  * cg_out (may be NULL) receives the final parameter vector (ma values). */
 int pso_fit(pso_problem* p, double freq, int m, double* out, double* cg_out);
 

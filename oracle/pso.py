@@ -128,10 +128,10 @@ class Oracle:
         return out
 
     def fit(self, freq: float, pole: int):
-        out = np.zeros(9)
+        out = np.zeros(10)
         cg = np.zeros(self.ma)
         lib().pso_fit(self.h, float(freq), int(pole), _p(out), _p(cg))
-        keys = ("dev", "dark", "totarea", "period_d", "lambda_deg", "beta_deg", "chisq", "niter", "alamda")
+        keys = ("dev", "dark", "totarea", "period_d", "lambda_deg", "beta_deg", "chisq", "niter", "alamda", "status")
         return dict(zip(keys, out.tolist())), cg
 
     def mrqcof(self, a):

@@ -73,7 +73,9 @@ def test_fits_match_oracle(native, oracle_lib, name):
             ro, _ = o.fit(f, pole)
             rg = g.fit(f, pole)
             assert rg["niter"] == int(ro["niter"])
-            assert rg["status"] == 0
+            # a singular damped system freezes the fit in both (gauss_errc.c:45-50,
+            # mrqmin.c:61); all-relative inputs with free phase parameters do that
+            assert rg["status"] == int(ro["status"])
             e = abs(rg["chisq"] - ro["chisq"]) / abs(ro["chisq"])
             worst = max(worst, e)
             assert e <= FIT_TOL, (name, n, pole, rg["chisq"], ro["chisq"])
