@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stdint.h>
 
 namespace psb {
 
@@ -27,6 +28,11 @@ struct DevProblem {
     const int* free_idx; // [mfit] parameter index of each free parameter
     const double* cg_first;  // [C]
     const double* pole0;     // [10][2]: initial beta' and lambda [rad]
+    // mixed-precision form only
+    const float* fac32;          // [F][4]: nx, ny, nz, 0 (FP32 copies)
+    const uint16_t* bsw;         // [nchunk][2][64 x 64] BF16 hi/lo of Dsph, swizzled K-major tiles
+    int nchunk;                  // facet chunks of 64 (F padded up)
+    int* err;                    // device error word (bounded waits that gave up)
     // scalars
     double phi0, conw_r, alamda_start, alamda_incr, log_cl, par1, par2, par3, ndata_m3;
     double freq_start, freq_step;
@@ -69,6 +75,14 @@ int fp64_max_blocks_per_sm(const DevProblem& P, int* threads);
 // P is the host copy (sizes, launch shape); dP the same struct in device memory.
 cudaError_t launch_fp64_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s);
 cudaError_t launch_fp64_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s);
+// Mixed-precision form (ps_mixed.cu).  The J scratch holds FP32 columns
+// (ma x npad floats) followed by the FP64 model values (npad doubles).
+size_t mixed_smem_bytes(const DevProblem& P);
+int mixed_max_blocks_per_sm(const DevProblem& P, int* threads);
+cudaError_t launch_mixed_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s);
+cudaError_t launch_mixed_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s);
+inline long long mixed_scratch_doubles(const DevProblem& P) { return ((long long)P.ma * P.npad + 1) / 2 + P.npad; }
+
 cudaError_t launch_period_reduce(const FitOut* fits, int n_periods, double ndata_m3, int prepass,
                                  void* records /* ps_record[n_periods] */, cudaStream_t s);
 
