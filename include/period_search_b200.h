@@ -123,6 +123,20 @@ int ps_scan(ps_ctx* ctx, int n_from, int n_to, ps_record* out);
  * Used to time the scan with inputs and outputs resident in HBM. */
 int ps_scan_device(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, void* stream);
 
+/* ps_scan_device without any device-memory allocation.  No counterpart in
+ * the reference: it exists for callers that cannot allocate while they scan
+ * (work recorded into a CUDA graph, a fixed pre-sized memory budget, a plugin
+ * inside a process whose allocator it does not own).  Set the context up
+ * first (ps_open*, then ps_precalc or ps_set_conw_r, which allocate); this
+ * call then takes all scratch from one 64 MiB device array that the library
+ * holds on every GPU it runs on until exit, and rejects, with PS_ERR_LIMIT, a
+ * period range whose 72 bytes per fit plus one CTA's Jacobian scratch do not
+ * fit in it.  Asynchronous on `stream` (NULL = the context's stream).  All
+ * calls share the array: calls that overlap on the GPU race, so serialise
+ * them.  The first call on a device looks up the array's device address;
+ * make it before any stream capture.  FP64 form only. */
+int ps_scan_device_noalloc(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, void* stream);
+
 /* One LM fit at trial frequency freq [1/day] from initial pole m (1..10)
  * (period_search_BOINC.cpp:817-920).  cg_out (may be NULL) receives the
  * final parameter vector (ma values). */

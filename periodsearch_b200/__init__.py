@@ -110,7 +110,7 @@ _lib = None
 EXPORTS = (
     "ps_open_file", "ps_open", "ps_close", "ps_precalc", "ps_set_conw_r", "ps_n_periods", "ps_scan",
     "ps_scan_device", "ps_fit", "ps_mrqcof", "ps_model", "ps_info", "ps_get_array", "ps_open_host_only",
-    "ps_format_record", "ps_last_error", "ps_kernel_launches",
+    "ps_format_record", "ps_last_error", "ps_kernel_launches", "ps_scan_device_noalloc",
 )
 
 
@@ -134,6 +134,7 @@ def load_library(path: str | None = None):
         "ps_n_periods": (ctypes.c_int, [vp]),
         "ps_scan": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp]),
         "ps_scan_device": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
+        "ps_scan_device_noalloc": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, vp, vp]),
         "ps_fit": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_FitResult), _D]),
         "ps_mrqcof": (ctypes.c_int, [vp, _D, _D, _D, _D]),
         "ps_model": (ctypes.c_int, [vp, _D, _D, _D]),

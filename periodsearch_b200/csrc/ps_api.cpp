@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/period_search_b200.h"
+#include "ps_ctx.hpp"
 #include "ps_device.hpp"
 #include "ps_host.hpp"
 
@@ -33,60 +34,22 @@ int cuda_fail(cudaError_t e, const char* where) {
     return PS_ERR_CUDA;
 }
 
+}  // namespace
+
+namespace psb {
+int set_error(int code, const std::string& msg) { return fail(code, msg); }
+void count_launch() { g_launches++; }
+}  // namespace psb
+
+namespace {
+
+using psb::DevBuf;
+
 #define PSB_CUDA(call)                                  \
     do {                                                \
         cudaError_t e_ = (call);                        \
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
-
-template <class T>
-struct DevBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    cudaError_t ensure(size_t count) {
-        if (count <= n) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-        if (e == cudaSuccess) n = count;
-        return e;
-    }
-    cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
-        cudaError_t e = ensure(v.size() ? v.size() : 1);
-        if (e != cudaSuccess || v.empty()) return e;
-        return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
-    }
-    void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-};
-
-}  // namespace
-
-struct ps_ctx {
-    Problem prob;
-    int device = 0;
-    int form = PS_FORM_FP64;
-    bool host_only = true;
-    bool rows_ready = false;
-    cudaStream_t stream = nullptr;
-    int sms = 0, blocks_per_sm = 0;
-    psb::DevProblem dp{};
-    // device tables
-    DevBuf<double> d_pts, d_rows, d_fac, d_dsph, d_cpl, d_cfc, d_cfs, d_cgf, d_pole;
-    DevBuf<int> d_lc, d_free, d_queue;
-    DevBuf<double> d_scratch;
-    DevBuf<psb::FitOut> d_fits;
-    DevBuf<ps_record> d_rec;
-    DevBuf<double> d_eval;
-    DevBuf<psb::DevProblem> d_dp;
-    std::vector<int> free_idx;
-};
-
-namespace {
 
 // Stop rule as the reference sets it up per fit (period_search_BOINC.cpp:846-859).
 void stop_rule(Problem& p, int& n_iter_max, double& iter_diff_max, int& n_iter_min) {

@@ -1,0 +1,68 @@
+// Private definition of the C ABI's context (ps_ctx) and its device
+// buffers, shared by the translation units that implement the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/period_search_b200.h"
+#include "ps_device.hpp"
+#include "ps_host.hpp"
+
+namespace psb {
+
+// Records the message returned by ps_last_error() for the calling thread.
+int set_error(int code, const std::string& msg);
+// Counts one kernel launch for ps_kernel_launches().
+void count_launch();
+
+// Grow-only device buffer.
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(size_t count) {
+        if (count <= n) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        return e;
+    }
+    cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
+        cudaError_t e = ensure(v.size() ? v.size() : 1);
+        if (e != cudaSuccess || v.empty()) return e;
+        return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+}  // namespace psb
+
+struct ps_ctx {
+    psb::Problem prob;
+    int device = 0;
+    int form = PS_FORM_FP64;
+    bool host_only = true;
+    bool rows_ready = false;
+    cudaStream_t stream = nullptr;
+    int sms = 0, blocks_per_sm = 0;
+    psb::DevProblem dp{};
+    // device tables
+    psb::DevBuf<double> d_pts, d_rows, d_fac, d_dsph, d_cpl, d_cfc, d_cfs, d_cgf, d_pole;
+    psb::DevBuf<int> d_lc, d_free, d_queue;
+    psb::DevBuf<double> d_scratch;
+    psb::DevBuf<psb::FitOut> d_fits;
+    psb::DevBuf<ps_record> d_rec;
+    psb::DevBuf<double> d_eval;
+    psb::DevBuf<psb::DevProblem> d_dp;
+    std::vector<int> free_idx;
+};
+
