@@ -163,6 +163,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--periods-per-step", type=int, default=592)
+    ap.add_argument("--form", default="fp64", choices=["fp64", "fast", "mixed"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--profile", action="store_true",
@@ -199,7 +200,8 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    g = ps.PeriodSearch(path, device=local)
+    form = {"fp64": ps.PS_FORM_FP64, "fast": ps.PS_FORM_FAST, "mixed": ps.PS_FORM_MIXED}[args.form]
+    g = ps.PeriodSearch(path, device=local, form=form)
     # convexity-weight pre-pass (100 fits per round), timed on its own
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -259,7 +261,7 @@ def main():
         a, b = batch(args.warmup + s)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        h = ps.PeriodSearch(desc=desc, device=local)
+        h = ps.PeriodSearch(desc=desc, device=local, form=form)
         h.set_conw_r(conw_r)
         rec_host = h.scan(a, b)
         h.close()
@@ -288,13 +290,14 @@ def main():
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "peak_source": peak_src, "traffic": None,
                 "fp64_nominal_tflops": 37.0, "frac_of_fp64_nominal": achieved / 37.0,
-                "kernel": "fit_kernel<56> (FP64 form: DFMA pipe, not tensor cores)",
+                "kernel": {"fp64": "fit_kernel<56,false> (FP64 pipe, no FMA by design)", "fast": "fit_kernel<56,true> (FP64 pipe, fused)", "mixed": "mixed_fit_kernel (FP64/FP32 SIMT + tcgen05 shape block)"}[args.form],
                 "flop_per_launch": flop_launch}
     line = {
         "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": "fp64 (drop-in)", "periods_per_step": B,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+bf16x3" if args.form == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "form": {"fp64": "fp64 (drop-in, reference operation order)", "fast": "fast fp64 (rearranged, fused; rounding-level differences)", "mixed": "mixed (FP64 model/solve, FP32 derivatives, tcgen05 split-BF16 shape block)"}[args.form], "periods_per_step": B,
                    "fits_per_step": fits_per_step, "l2": "flushed (256 MB write) between timed steps",
                    "prepass": {"fits": None, "seconds": prepass_s, "conw_r": conw_r},
                    "parallelism": f"period shards x{world}"},

@@ -33,6 +33,18 @@
 #define PSO_N_POLES 10              /* constants.h:11 */
 #define LM1 (PSO_MAX_LM + 1)
 
+/* Perturbed builds for the chaotic-period triage (oracle/Makefile targets
+   libps_oracle_sq.so / libps_oracle_fma.so / ps_oracle_sq / ps_oracle_fma):
+   PSO_SQUARE_BY_MUL replaces pow(x, 2) on the fit path by x*x (it differs
+   from glibc's pow in ~0.1 % of calls by one ulp).  The default build uses
+   pow exactly like the reference. */
+#ifdef PSO_SQUARE_BY_MUL
+static double sq2(double x) { return x * x; }
+#define PSO_SQ(x) sq2(x)
+#else
+#define PSO_SQ(x) pow((x), 2)
+#endif
+
 struct pso_problem {
     /* input header, period_search_BOINC.cpp:277-303 */
     double per_start, per_step_coef, per_end;
@@ -544,8 +556,8 @@ static double bright(pso_problem* p, const double ee[4], const double ee0[4], do
             dnom = mu[i] + mu0[i];
             s[i] = mu[i] * mu0[i] * (cl + cls / dnom);
             br = br + p->area[i] * s[i];
-            dsmu[i] = cls * pow(mu0[i] / dnom, 2) + cl * mu0[i];
-            dsmu0[i] = cls * pow(mu[i] / dnom, 2) + cl * mu[i];
+            dsmu[i] = cls * PSO_SQ(mu0[i] / dnom) + cl * mu0[i];
+            dsmu0[i] = cls * PSO_SQ(mu[i] / dnom) + cl * mu[i];
             dbr[i] = p->darea[i] * s[i];
         }
     }
@@ -1140,7 +1152,7 @@ static void run_fit(pso_problem* p, double freq, int m, double* out) {
                 chck[i] = 0;
                 for (j = 1; j <= p->numfac; j++) chck[i] = chck[i] + p->area[j] * NOR(p, j, i);
             }
-            rchisq = p->chisq - (pow(chck[1], 2) + pow(chck[2], 2) + pow(chck[3], 2)) * pow(p->conw_r, 2);
+            rchisq = p->chisq - (PSO_SQ(chck[1]) + PSO_SQ(chck[2]) + PSO_SQ(chck[3])) * PSO_SQ(p->conw_r);
         }
         dev_new = sqrt(rchisq / (p->ndata_tot - 3));
         if (dev_old - dev_new > 1e-10) {
@@ -1152,7 +1164,7 @@ static void run_fit(pso_problem* p, double freq, int m, double* out) {
        the reference (:900-902). */
     totarea = 0;
     for (i = 1; i <= p->numfac; i++) totarea = totarea + p->area[i];
-    sum = pow(chck[1], 2) + pow(chck[2], 2) + pow(chck[3], 2);
+    sum = PSO_SQ(chck[1]) + PSO_SQ(chck[2]) + PSO_SQ(chck[3]);
     dark = sqrt(sum);
     prd = 2 * PSO_PI / cg[Ncoef + 3];
     out[0] = dev_new;

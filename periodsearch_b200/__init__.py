@@ -37,6 +37,8 @@ EXE_PATH = os.path.join(_HERE, "period_search_b200")
 
 PS_OK, PS_ERR_IO, PS_ERR_LIMIT, PS_ERR_CUDA, PS_ERR_SINGULAR, PS_ERR_ARG, PS_ERR_DEVICE_LOOP = range(7)
 PS_FORM_FP64 = 0
+PS_FORM_MIXED = 1
+PS_FORM_FAST = 2
 
 RECORD_DTYPE = np.dtype(
     [("period_h", "f8"), ("rms", "f8"), ("chi2", "f8"), ("dark_pct", "f8"), ("lambda_deg", "f8"), ("beta_deg", "f8")]

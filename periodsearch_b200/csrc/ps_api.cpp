@@ -51,6 +51,66 @@ using psb::DevBuf;
         if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
     } while (0)
 
+// FP32 -> BF16, round to nearest even (finite inputs).
+uint16_t f2bf(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+float bf2f(uint16_t h) {
+    uint32_t u = (uint32_t)h << 16;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+
+// Tables of the mixed-precision form: FP32 facet normals and Dsph split into
+// BF16 hi/lo, laid out as the 128-byte-swizzled K-major tiles the tensor core
+// reads (per chunk of 64 facets: 64 coefficient rows x 64 facets, hi then lo).
+int upload_mixed(ps_ctx* c) {
+    const Problem& p = c->prob;
+    const int F = p.numfac, C = p.ncoef;
+    if (C > 64) return fail(PS_ERR_LIMIT, "the mixed form supports up to 64 shape coefficients (lmax <= 7)");
+    const int nchunk = (F + 63) / 64;
+    std::vector<float> fac32((size_t)F * 4, 0.f);
+    for (int f = 0; f < F; f++)
+        for (int k = 0; k < 3; k++) fac32[(size_t)f * 4 + k] = (float)p.nor[(size_t)f * 3 + k];
+    std::vector<uint16_t> bsw((size_t)nchunk * 2 * 64 * 64, 0);
+    for (int ch = 0; ch < nchunk; ch++) {
+        uint16_t* hi = &bsw[(size_t)ch * 2 * 4096];
+        uint16_t* lo = hi + 4096;
+        for (int n = 0; n < 64; n++)
+            for (int k = 0; k < 64; k++) {
+                const int f = ch * 64 + k;
+                const float v = (f < F && n < C) ? (float)p.dsph[(size_t)f * C + n] : 0.f;
+                const uint16_t h = f2bf(v);
+                const uint16_t l = f2bf(v - bf2f(h));
+                const size_t off = ((size_t)n * 128 + (((size_t)2 * k) ^ ((size_t)(n & 7) << 4))) / 2;
+                hi[off] = h;
+                lo[off] = l;
+            }
+    }
+    PSB_CUDA(c->d_fac32.upload(fac32, c->stream));
+    PSB_CUDA(c->d_bsw.upload(bsw, c->stream));
+    PSB_CUDA(c->d_err.ensure(1));
+    PSB_CUDA(cudaMemsetAsync(c->d_err.p, 0, sizeof(int), c->stream));
+    c->dp.fac32 = c->d_fac32.p;
+    c->dp.bsw = c->d_bsw.p;
+    c->dp.nchunk = nchunk;
+    c->dp.err = c->d_err.p;
+    return PS_OK;
+}
+
+// A bounded device wait that gave up shows up here after a synchronisation.
+int check_device_error(ps_ctx* c) {
+    if (c->form != PS_FORM_MIXED || !c->d_err.p) return PS_OK;
+    int e = 0;
+    PSB_CUDA(cudaMemcpy(&e, c->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) return fail(PS_ERR_DEVICE_LOOP, "a device wait on the tensor-core pipeline gave up (" + std::to_string(e) + ")");
+    return PS_OK;
+}
+
 // Stop rule as the reference sets it up per fit (period_search_BOINC.cpp:846-859).
 void stop_rule(Problem& p, int& n_iter_max, double& iter_diff_max, int& n_iter_min) {
     n_iter_max = 0;
@@ -196,7 +256,15 @@ int upload_static(ps_ctx* c) {
     d.freq_step = p.freq_step;
     stop_rule(p, d.n_iter_max, d.iter_diff_max, d.n_iter_min);
     int threads = 0;
-    c->blocks_per_sm = psb::fp64_max_blocks_per_sm(d, &threads);
+    if (c->form == PS_FORM_MIXED) {
+        int rc = upload_mixed(c);
+        if (rc) return rc;
+        c->blocks_per_sm = psb::mixed_max_blocks_per_sm(d, &threads);
+    } else if (c->form == PS_FORM_FAST) {
+        c->blocks_per_sm = psb::fast_max_blocks_per_sm(d, &threads);
+    } else {
+        c->blocks_per_sm = psb::fp64_max_blocks_per_sm(d, &threads);
+    }
     if (c->blocks_per_sm <= 0)
         return fail(PS_ERR_LIMIT, "fit kernel does not fit on the device (shared memory or registers)");
     return PS_OK;
@@ -235,8 +303,12 @@ int upload_rows(ps_ctx* c) {
     return PS_OK;
 }
 
+size_t scratch_stride(const ps_ctx* c) {
+    return c->form == PS_FORM_MIXED ? (size_t)psb::mixed_scratch_doubles(c->dp) : (size_t)(c->dp.ma + 1) * c->dp.npad;
+}
+
 int ensure_scratch(ps_ctx* c, int slots) {
-    const size_t stride = (size_t)(c->dp.ma + 1) * c->dp.npad;
+    const size_t stride = scratch_stride(c);
     PSB_CUDA(c->d_scratch.ensure(stride * slots));
     return PS_OK;
 }
@@ -257,8 +329,13 @@ int run_fits(ps_ctx* c, int n_from, int n_fits, int pole_override, double freq_o
     b.queue = c->d_queue.p;
     b.out = c->d_fits.p;
     b.scratch = c->d_scratch.p;
-    b.scratch_stride = (long long)(c->dp.ma + 1) * c->dp.npad;
-    PSB_CUDA(psb::launch_fp64_fits(c->dp, c->d_dp.p, b, grid, c->stream));
+    b.scratch_stride = (long long)scratch_stride(c);
+    if (c->form == PS_FORM_MIXED)
+        PSB_CUDA(psb::launch_mixed_fits(c->dp, c->d_dp.p, b, grid, c->stream));
+    else if (c->form == PS_FORM_FAST)
+        PSB_CUDA(psb::launch_fast_fits(c->dp, c->d_dp.p, b, grid, c->stream));
+    else
+        PSB_CUDA(psb::launch_fp64_fits(c->dp, c->d_dp.p, b, grid, c->stream));
     g_launches++;
     return PS_OK;
 }
@@ -313,7 +390,7 @@ int ps_open_host_only(const char* path, ps_ctx** out) {
 }
 
 int ps_open_file(const char* path, int device, int form, ps_ctx** out) {
-    if (form != PS_FORM_FP64) return fail(PS_ERR_ARG, "unknown form");
+    if (form != PS_FORM_FP64 && form != PS_FORM_MIXED && form != PS_FORM_FAST) return fail(PS_ERR_ARG, "unknown form");
     int rc = ps_open_host_only(path, out);
     if (rc) return rc;
     (*out)->form = form;
@@ -327,7 +404,7 @@ int ps_open_file(const char* path, int device, int form, ps_ctx** out) {
 
 int ps_open(const ps_problem_desc* d, int device, int form, ps_ctx** out) {
     if (!d || !out) return fail(PS_ERR_ARG, "null argument");
-    if (form != PS_FORM_FP64) return fail(PS_ERR_ARG, "unknown form");
+    if (form != PS_FORM_FP64 && form != PS_FORM_MIXED && form != PS_FORM_FAST) return fail(PS_ERR_ARG, "unknown form");
     *out = nullptr;
     if (d->n_points < 1 || d->n_lc < 1 || !d->lc_points || !d->lc_relative || !d->tim || !d->ee || !d->ee0 ||
         !d->brightness || !d->sig || !d->weight)
@@ -416,6 +493,9 @@ void ps_close(ps_ctx* c) {
         c->d_rec.release();
         c->d_eval.release();
         c->d_dp.release();
+        c->d_fac32.release();
+        c->d_bsw.release();
+        c->d_err.release();
         if (c->stream) cudaStreamDestroy(c->stream);
     }
     delete c;
@@ -442,6 +522,8 @@ int ps_precalc(ps_ctx* c, double* conw_r) {
         PSB_CUDA(cudaMemcpyAsync(rec.data(), c->d_rec.p, sizeof(ps_record) * max_test_periods,
                                  cudaMemcpyDeviceToHost, c->stream));
         PSB_CUDA(cudaStreamSynchronize(c->stream));
+        rc = check_device_error(c);
+        if (rc) return rc;
         for (int n = 0; n < max_test_periods; n++) sum_dark_facet = sum_dark_facet + rec[n].dark_pct;
         const double ave_dark_facet = sum_dark_facet / max_test_periods;
         if (ave_dark_facet < 1.0) new_conw = 1;
@@ -489,7 +571,7 @@ int ps_scan(ps_ctx* c, int n_from, int n_to, ps_record* out) {
     if (rc) return rc;
     PSB_CUDA(cudaMemcpyAsync(out, c->d_rec.p, sizeof(ps_record) * np, cudaMemcpyDeviceToHost, c->stream));
     PSB_CUDA(cudaStreamSynchronize(c->stream));
-    return PS_OK;
+    return check_device_error(c);
 }
 
 int ps_fit(ps_ctx* c, double freq, int pole, ps_fit_result* out, double* cg_out) {
@@ -502,6 +584,8 @@ int ps_fit(ps_ctx* c, double freq, int pole, ps_fit_result* out, double* cg_out)
     psb::FitOut o;
     PSB_CUDA(cudaMemcpyAsync(&o, c->d_fits.p, sizeof(o), cudaMemcpyDeviceToHost, c->stream));
     PSB_CUDA(cudaStreamSynchronize(c->stream));
+    rc = check_device_error(c);
+    if (rc) return rc;
     out->dev = o.dev;
     out->dark = o.dark;
     out->totarea = o.totarea;
@@ -523,7 +607,7 @@ static int run_eval(ps_ctx* c, const double* a, std::vector<double>& alpha, std:
     PSB_CUDA(cudaSetDevice(c->device));
     const psb::DevProblem& d = c->dp;
     const size_t na = d.ma, nal = (size_t)d.mfit * d.mfit, nb = d.mfit, ny = d.n_rows, nJ = (size_t)d.n_rows * d.ma;
-    const size_t scratch = (size_t)(d.ma + 1) * d.npad;
+    const size_t scratch = scratch_stride(c);
     const size_t total = na + nal + nb + 1 + ny + nJ + scratch;
     PSB_CUDA(c->d_eval.ensure(total));
     double* base = c->d_eval.p;
@@ -536,7 +620,12 @@ static int run_eval(ps_ctx* c, const double* a, std::vector<double>& alpha, std:
     E.J = E.y + ny;
     E.scratch = E.J + nJ;
     PSB_CUDA(cudaMemcpyAsync(base, a, na * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    PSB_CUDA(psb::launch_fp64_eval(d, c->d_dp.p, E, c->stream));
+    if (c->form == PS_FORM_MIXED)
+        PSB_CUDA(psb::launch_mixed_eval(d, c->d_dp.p, E, c->stream));
+    else if (c->form == PS_FORM_FAST)
+        PSB_CUDA(psb::launch_fast_eval(d, c->d_dp.p, E, c->stream));
+    else
+        PSB_CUDA(psb::launch_fp64_eval(d, c->d_dp.p, E, c->stream));
     g_launches++;
     alpha.resize(nal);
     beta.resize(nb);
@@ -552,7 +641,7 @@ static int run_eval(ps_ctx* c, const double* a, std::vector<double>& alpha, std:
         PSB_CUDA(cudaMemcpyAsync(J->data(), E.J, nJ * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     }
     PSB_CUDA(cudaStreamSynchronize(c->stream));
-    return PS_OK;
+    return check_device_error(c);
 }
 
 int ps_mrqcof(ps_ctx* c, const double* a, double* alpha, double* beta, double* chisq) {

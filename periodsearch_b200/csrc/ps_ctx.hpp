@@ -63,6 +63,9 @@ struct ps_ctx {
     psb::DevBuf<ps_record> d_rec;
     psb::DevBuf<double> d_eval;
     psb::DevBuf<psb::DevProblem> d_dp;
+    psb::DevBuf<float> d_fac32;
+    psb::DevBuf<uint16_t> d_bsw;
+    psb::DevBuf<int> d_err;
     std::vector<int> free_idx;
 };
 

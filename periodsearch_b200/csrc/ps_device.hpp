@@ -75,6 +75,12 @@ int fp64_max_blocks_per_sm(const DevProblem& P, int* threads);
 // P is the host copy (sizes, launch shape); dP the same struct in device memory.
 cudaError_t launch_fp64_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s);
 cudaError_t launch_fp64_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s);
+// Fast FP64 form (ps_fast.cu): same launch interface as the FP64 form.
+size_t fast_smem_bytes(const DevProblem& P);
+int fast_max_blocks_per_sm(const DevProblem& P, int* threads);
+cudaError_t launch_fast_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s);
+cudaError_t launch_fast_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s);
+
 // Mixed-precision form (ps_mixed.cu).  The J scratch holds FP32 columns
 // (ma x npad floats) followed by the FP64 model values (npad doubles).
 size_t mixed_smem_bytes(const DevProblem& P);

@@ -11,6 +11,8 @@
 
 namespace psb {
 namespace fitcommon {
+// internal linkage: each kernel file gets its own copy
+namespace {
 
 constexpr int kThreads = 256;
 constexpr double kPiD = 3.14159265358979323846;
@@ -225,5 +227,6 @@ __device__ void entry_map(int mfit, int* ent) {
 }
 
 
+}  // namespace
 }  // namespace fitcommon
 }  // namespace psb

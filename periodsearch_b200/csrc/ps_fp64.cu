@@ -37,499 +37,11 @@
 
 #include "ps_device.hpp"
 #include "ps_fit_common.cuh"
+#include "ps_fit_impl.cuh"
 
 namespace psb {
 
 namespace {
-
-using namespace fitcommon;
-
-constexpr int kFch = 32;     // facets per shared-memory chunk
-constexpr int kRt = 32;      // rows per alpha tile
-constexpr int kMaxEpt = 16;  // alpha/beta/chi2 entries per thread
-
-// Shared-memory layout, offsets in doubles.
-struct Layout {
-    int cg, atry, alpha, covar, beta, da, g, area, dres, dave, blm, misc, red, work, ipiv, ent;
-    size_t bytes;
-};
-
-__host__ __device__ inline Layout make_layout(const DevProblem& P) {
-    Layout L;
-    int o = 0;
-#define PSB_TAKE(field, n) \
-    L.field = o;           \
-    o += ((n) + 1) & ~1;
-    PSB_TAKE(cg, P.ma)
-    PSB_TAKE(atry, P.ma)
-    PSB_TAKE(alpha, P.mfit * P.mfit)
-    PSB_TAKE(covar, P.mfit * P.mfit)
-    PSB_TAKE(beta, P.mfit)
-    PSB_TAKE(da, P.mfit)
-    PSB_TAKE(g, P.F)
-    PSB_TAKE(area, P.F)
-    PSB_TAKE(dres, 3 * P.C)
-    PSB_TAKE(dave, P.ma + 2)
-    PSB_TAKE(blm, 28)
-    PSB_TAKE(misc, 32)
-    PSB_TAKE(red, 2 * (kThreads / 32) + 2)
-    int chunk = kFch * 5 + kFch * P.NCB;
-    int tile = kRt * (P.mfit + 1) + kRt * (P.mfit + 2);
-    int w = chunk > tile ? chunk : tile;
-    if (P.mfit + 2 > w) w = P.mfit + 2;
-    PSB_TAKE(work, w)
-#undef PSB_TAKE
-    L.ipiv = o;
-    L.ent = o + (P.mfit + 2 + 1) / 2;  // int offset counted in doubles
-    const int nent = P.mfit * (P.mfit + 1) / 2 + P.mfit + 1;
-    L.bytes = (size_t)L.ent * sizeof(double) + (size_t)nent * sizeof(int);
-    return L;
-}
-
-// slots of the misc area
-enum {
-    M_CHISQ = 0,  // chi2 of the evaluation just done
-    M_CHK0 = 1,   // its convexity residuals (3)
-    M_SAREA = 4,  // its facet-area sum
-    M_CL = 5,
-    M_CLS = 6,
-    M_OMG = 7,
-    M_P1 = 8,
-    M_P2 = 9,
-    M_P3 = 10,
-    M_WORK = 11
-};
-
-// One model evaluation, the reference's mrqcof (mrqcof.c:16-148) at
-// parameters a (shared memory).  Writes the symmetrised alpha and beta into
-// alpha_out / beta_out (shared memory) and chi2, the convexity residuals
-// (= the driver's chck, period_search_BOINC.cpp:876-880) and the facet-area
-// sum into misc.  J^T (ma columns of npad rows) and y go to the CTA's
-// scratch.  All threads enter and leave together.
-template <int NCB>
-__device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double* sm, const double* a,
-                                      double* alpha_out, double* beta_out, double* Jt, double* yt) {
-    const DevProblem& P = *Pp;
-    const Layout L = make_layout(P);
-    const int* ent = (const int*)(sm + L.ent);
-    const int nent = P.mfit * (P.mfit + 1) / 2 + P.mfit + 1;
-    const int tid = threadIdx.x;
-    const int F = P.F, C = P.C, ma = P.ma, npad = P.npad, mfit = P.mfit;
-    double* g = sm + L.g;
-    double* area = sm + L.area;
-    double* misc = sm + L.misc;
-    double* B = sm + L.blm;
-    double* D = sm + L.blm + 9;
-    double* dres = sm + L.dres;
-    double* work = sm + L.work;
-
-    // blmatrix (mrqcof.c:34) and the per-evaluation scalars of bright.c:26-33
-    if (tid == 0) {
-        blmatrix(a[C], a[C + 1], B, D);
-        misc[M_CL] = exp(a[C + 6]);
-        misc[M_CLS] = a[C + 7];
-        misc[M_OMG] = a[C + 2];
-        misc[M_P1] = a[C + 3];
-        misc[M_P2] = a[C + 4];
-        misc[M_P3] = a[C + 5];
-    }
-    // curv.c:15-37: g = exp(sum over (m, l) of Pleg * (c*Fc + s*Fs))
-    for (int f = tid; f < F; f += kThreads) {
-        const double* pl = P.cpl + (size_t)f * P.nq;
-        const double* fc = P.cfc + (size_t)f * (P.mmax + 1);
-        const double* fs = P.cfs + (size_t)f * (P.mmax + 1);
-        double gi = 0;
-        int n = 0, q = 0;
-        for (int m = 0; m <= P.mmax; m++) {
-            const double fcm = fc[m], fsm = fs[m];
-            for (int l = m; l <= P.lmax; l++) {
-                double fsum = a[n] * fcm;
-                n++;
-                if (m != 0) {
-                    fsum = fsum + a[n] * fsm;
-                    n++;
-                }
-                gi = gi + pl[q] * fsum;
-                q++;
-            }
-        }
-        gi = exp(gi);
-        g[f] = gi;
-        area[f] = P.fac[(size_t)f * 4 + 3] * gi;
-    }
-    __syncthreads();
-    // Sequential facet sums: chck / conv residuals (conv.c:22-27), the
-    // facet-area sum (period_search_BOINC.cpp:900-902) and the conv-row shape
-    // derivatives, one thread per sum, facets in order.
-    for (int job = tid; job < 4 + 3 * C; job += kThreads) {
-        double s = 0;
-        if (job < 3) {
-            for (int f = 0; f < F; f++) s = s + area[f] * P.fac[(size_t)f * 4 + job];
-            misc[M_CHK0 + job] = s;
-        } else if (job == 3) {
-            for (int f = 0; f < F; f++) s = s + area[f];
-            misc[M_SAREA] = s;
-        } else {
-            const int nc = (job - 4) / C, j = (job - 4) - nc * C;
-            for (int f = 0; f < F; f++) {
-                const double dg = g[f] * P.dsph[(size_t)f * NCB + j];
-                s += P.fac[(size_t)f * 4 + 3] * dg * P.fac[(size_t)f * 4 + nc];
-            }
-            dres[nc * C + j] = s;
-        }
-    }
-    // bright.c:54-125 for every data point
-    double* s_fac = work;
-    double* s_dg = work + kFch * 5;
-    const double cl = misc[M_CL], cls = misc[M_CLS];
-    for (int base = 0; base < P.n_points; base += kThreads) {
-        const int p = base + tid;
-        const bool act = p < P.n_points;
-        PointGeom G;
-        if (act) point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
-        double acc[NCB];
-#pragma unroll
-        for (int k = 0; k < NCB; k++) acc[k] = 0;
-        double br = 0, rot0 = 0, rot1 = 0, rot2 = 0, s_cl = 0, s_cls = 0;
-        for (int f0 = 0; f0 < F; f0 += kFch) {
-            const int nf = min(kFch, F - f0);
-            __syncthreads();
-            for (int idx = tid; idx < nf * NCB; idx += kThreads) {
-                const int ff = idx / NCB, k = idx - ff * NCB;
-                s_dg[idx] = g[f0 + ff] * P.dsph[(size_t)(f0 + ff) * NCB + k];
-            }
-            for (int ff = tid; ff < nf; ff += kThreads) {
-                const double* fa = P.fac + (size_t)(f0 + ff) * 4;
-                s_fac[ff * 5 + 0] = fa[0];
-                s_fac[ff * 5 + 1] = fa[1];
-                s_fac[ff * 5 + 2] = fa[2];
-                s_fac[ff * 5 + 3] = area[f0 + ff];
-                s_fac[ff * 5 + 4] = fa[3];
-            }
-            __syncthreads();
-            if (act) {
-                for (int ff = 0; ff < nf; ff++) {
-                    const double nx = s_fac[ff * 5 + 0], ny = s_fac[ff * 5 + 1], nz = s_fac[ff * 5 + 2];
-                    const double mu = G.e[0] * nx + G.e[1] * ny + G.e[2] * nz;
-                    const double mu0 = G.e0[0] * nx + G.e0[1] * ny + G.e0[2] * nz;
-                    if ((mu > kTinyD) && (mu0 > kTinyD)) {
-                        const double ar = s_fac[ff * 5 + 3], darea = s_fac[ff * 5 + 4];
-                        const double dnom = mu + mu0;
-                        const double s = mu * mu0 * (cl + cls / dnom);
-                        br = br + ar * s;
-                        const double q0 = mu0 / dnom, q1 = mu / dnom;
-                        const double dsmu = cls * (q0 * q0) + cl * mu0;
-                        const double dsmu0 = cls * (q1 * q1) + cl * mu;
-                        const double dbr = darea * s;
-                        const double* dg = s_dg + ff * NCB;
-#pragma unroll
-                        for (int k = 0; k < NCB; k++) acc[k] = acc[k] + dbr * dg[k];
-                        {
-                            const double sum = nx * G.de[0][0] + ny * G.de[1][0] + nz * G.de[2][0];
-                            const double sum0 = nx * G.de0[0][0] + ny * G.de0[1][0] + nz * G.de0[2][0];
-                            rot0 = rot0 + ar * (dsmu * sum + dsmu0 * sum0);
-                        }
-                        {
-                            const double sum = nx * G.de[0][1] + ny * G.de[1][1] + nz * G.de[2][1];
-                            const double sum0 = nx * G.de0[0][1] + ny * G.de0[1][1] + nz * G.de0[2][1];
-                            rot1 = rot1 + ar * (dsmu * sum + dsmu0 * sum0);
-                        }
-                        {
-                            const double sum = nx * G.de[0][2] + ny * G.de[1][2] + nz * G.de[2][2];
-                            const double sum0 = nx * G.de0[0][2] + ny * G.de0[1][2] + nz * G.de0[2][2];
-                            rot2 = rot2 + ar * (dsmu * sum + dsmu0 * sum0);
-                        }
-                        s_cl = s_cl + mu * mu0 * ar;
-                        s_cls = s_cls + ar * mu * mu0 / (mu + mu0);
-                    }
-                }
-            }
-        }
-        if (act) {
-            const double sc = G.scale;
-#pragma unroll
-            for (int k = 0; k < NCB; k++)
-                if (k < C) Jt[(size_t)k * npad + p] = sc * acc[k];
-            Jt[(size_t)(C + 0) * npad + p] = sc * rot0;
-            Jt[(size_t)(C + 1) * npad + p] = sc * rot1;
-            Jt[(size_t)(C + 2) * npad + p] = sc * rot2;
-            Jt[(size_t)(C + 3) * npad + p] = br * G.dphp[0];
-            Jt[(size_t)(C + 4) * npad + p] = br * G.dphp[1];
-            Jt[(size_t)(C + 5) * npad + p] = br * G.dphp[2];
-            Jt[(size_t)(C + 6) * npad + p] = sc * s_cl * cl;
-            Jt[(size_t)(C + 7) * npad + p] = sc * s_cls;
-            yt[p] = br * sc;
-        }
-    }
-    __syncthreads();
-    // convexity rows (conv.c:12-29): y = residual, J = dres for the shape
-    // coefficients and 0 elsewhere
-    for (int job = tid; job < 3 * ma; job += kThreads) {
-        const int nc = job / ma, l = job - nc * ma;
-        const int row = P.n_points + nc;
-        Jt[(size_t)l * npad + row] = l < C ? dres[nc * C + l] : 0.0;
-        if (l == 0) yt[row] = misc[M_CHK0 + nc];
-    }
-    __syncthreads();
-    // relative-lightcurve normalisation (mrqcof.c:53-58, 75-83, 92-104)
-    double* dave = sm + L.dave;
-    for (int lc = 0; lc < P.n_lc; lc++) {
-        if (!P.lc_rel[lc]) continue;
-        const int r0 = P.lc_start[lc], r1 = P.lc_start[lc + 1];
-        for (int job = tid; job <= ma; job += kThreads) {
-            const double* col = job < ma ? Jt + (size_t)job * npad : yt;
-            double s = 0;
-            for (int r = r0; r < r1; r++) s = s + col[r];
-            dave[job] = s;
-        }
-        __syncthreads();
-        const double ave = dave[ma];
-        const double lpts = (double)P.lc_npts[lc];
-        for (int r = r0 + tid; r < r1; r += kThreads) {
-            const double coef = P.sig[r] * lpts / ave;
-            const double y = yt[r];
-            for (int l = 0; l < ma; l++) {
-                double* d = Jt + (size_t)l * npad + r;
-                *d = coef * (*d - y * dave[l] / ave);
-            }
-            yt[r] = coef * y;
-            Jt[r] = 0;
-        }
-        __syncthreads();
-    }
-    // alpha = J^T W J, beta = J^T W dy, chi2 (mrqcof.c:106-147), rows in
-    // order.  Tile: Ws[r][j] = (J[r][l_j] sig2i) wght (j < mfit),
-    // Ws[r][mfit] = dy dy sig2i wght; Js[r][k] = J[r][l_k] (k < mfit),
-    // Js[r][mfit] = dy, Js[r][mfit+1] = 1.
-    double* Ws = work;
-    double* Js = work + kRt * (mfit + 1);
-    const int wst = mfit + 1, jst = mfit + 2;
-    double acc2[kMaxEpt];
-#pragma unroll
-    for (int s = 0; s < kMaxEpt; s++) acc2[s] = 0;
-    for (int r0 = 0; r0 < P.n_rows; r0 += kRt) {
-        const int nr = min(kRt, P.n_rows - r0);
-        __syncthreads();
-        for (int idx = tid; idx < nr * mfit; idx += kThreads) {
-            const int j = idx / nr, r = idx - j * nr;
-            const int row = r0 + r;
-            const double d = Jt[(size_t)P.free_idx[j] * npad + row];
-            Js[r * jst + j] = d;
-            Ws[r * wst + j] = d * P.sig2i[row] * P.wght[row];
-        }
-        for (int r = tid; r < nr; r += kThreads) {
-            const int row = r0 + r;
-            const double dy = P.yobs[row] - yt[row];
-            Js[r * jst + mfit] = dy;
-            Js[r * jst + mfit + 1] = 1.0;
-            Ws[r * wst + mfit] = dy * dy * P.sig2i[row] * P.wght[row];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int s = 0; s < kMaxEpt; s++) {
-            const int e = tid + s * kThreads;
-            if (e < nent) {
-                const int pk = ent[e];
-                const double* w = Ws + (pk & 0xffff);
-                const double* jj = Js + (pk >> 16);
-                double acc = acc2[s];
-                for (int r = 0; r < nr; r++) acc = acc + w[r * wst] * jj[r * jst];
-                acc2[s] = acc;
-            }
-        }
-    }
-#pragma unroll
-    for (int s = 0; s < kMaxEpt; s++) {
-        const int e = tid + s * kThreads;
-        if (e < nent) {
-            const int j = ent[e] & 0xffff, k = ent[e] >> 16;
-            if (k < mfit) {
-                alpha_out[j * mfit + k] = acc2[s];
-                alpha_out[k * mfit + j] = acc2[s];
-            } else if (j < mfit) {
-                beta_out[j] = acc2[s];
-            } else {
-                misc[M_CHISQ] = acc2[s];
-            }
-        }
-    }
-    __syncthreads();
-}
-
-template <int NCB>
-__global__ void __launch_bounds__(kThreads, 1) fit_kernel(const DevProblem* __restrict__ Pp, FitBatch Bt) {
-    extern __shared__ __align__(16) double sm[];
-    const DevProblem& P = *Pp;
-    const Layout L = make_layout(P);
-    const int tid = threadIdx.x;
-    const int C = P.C, ma = P.ma, mfit = P.mfit;
-    double* cg = sm + L.cg;
-    double* atry = sm + L.atry;
-    double* misc = sm + L.misc;
-    int* ipiv = (int*)(sm + L.ipiv);
-    double* Jt = Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride;
-    double* yt = Jt + (size_t)ma * P.npad;
-    entry_map(mfit, (int*)(sm + L.ent));
-
-    for (;;) {
-        __syncthreads();
-        if (tid == 0) misc[M_WORK] = (double)atomicAdd(Bt.queue, 1);
-        __syncthreads();
-        const int w = (int)misc[M_WORK];
-        if (w >= Bt.n_fits) break;
-        double freq;
-        int pole;
-        if (Bt.pole_override) {
-            freq = Bt.freq_override;
-            pole = Bt.pole_override;
-        } else {
-            const int n = Bt.n_from + w / 10;
-            pole = w % 10 + 1;
-            freq = P.freq_start - (n - 1) * P.freq_step;
-        }
-        // initial parameters, period_search_BOINC.cpp:819-844
-        for (int i = tid; i < ma; i += kThreads) {
-            double v;
-            if (i < C)
-                v = P.cg_first[i];
-            else if (i == C)
-                v = P.pole0[(pole - 1) * 2];
-            else if (i == C + 1)
-                v = P.pole0[(pole - 1) * 2 + 1];
-            else if (i == C + 2) {
-                const double prd = 1 / freq;
-                v = 24 * 2 * kPiD / prd;
-            } else if (i == C + 3)
-                v = P.par1;
-            else if (i == C + 4)
-                v = P.par2;
-            else if (i == C + 5)
-                v = P.par3;
-            else if (i == C + 6)
-                v = P.log_cl;
-            else
-                v = 1;
-            cg[i] = v;
-        }
-        __syncthreads();
-        // Levenberg-Marquardt loop, period_search_BOINC.cpp:846-893, with
-        // mrqmin (mrqmin.c:11-110) inlined.  Scalars are kept identically in
-        // every thread.
-        double* alpha = sm + L.alpha;
-        double* covar = sm + L.covar;
-        double* beta = sm + L.beta;
-        double* da = sm + L.da;
-        double alamda = -1, ochisq = 0, chisq = 0, iter_diff = 1e40, dev_old = 1e30, dev_new = 0, rchisq = -1;
-        double chk0 = 0, chk1 = 0, chk2 = 0, cur0 = 0, cur1 = 0, cur2 = 0, s_cur = 0, s_last = 0;
-        int niter = 0, status = 0;
-        while (((niter < P.n_iter_max) && (iter_diff > P.iter_diff_max)) || (niter < P.n_iter_min)) {
-            if (alamda < 0) {
-                alamda = P.alamda_start;
-                evaluate<NCB>(Pp, sm, cg, alpha, beta, Jt, yt);
-                ochisq = misc[M_CHISQ];
-                cur0 = misc[M_CHK0];
-                cur1 = misc[M_CHK0 + 1];
-                cur2 = misc[M_CHK0 + 2];
-                s_cur = s_last = misc[M_SAREA];
-                for (int i = tid; i < ma; i += kThreads) atry[i] = cg[i];
-            }
-            for (int idx = tid; idx < mfit * mfit; idx += kThreads) {
-                const int j = idx / mfit, k = idx - j * mfit;
-                covar[idx] = (j == k) ? alpha[idx] * (1 + alamda) : alpha[idx];
-            }
-            for (int j = tid; j < mfit; j += kThreads) da[j] = beta[j];
-            __syncthreads();
-            const int err = gauss_jordan(covar, da, mfit, ipiv, sm + L.work, sm + L.red);
-            __syncthreads();
-            if (err == 0) {
-                for (int j = tid; j < mfit; j += kThreads) {
-                    const int l = P.free_idx[j];
-                    atry[l] = cg[l] + da[j];
-                }
-                __syncthreads();
-                evaluate<NCB>(Pp, sm, atry, covar, da, Jt, yt);
-                const double temp = misc[M_CHISQ];
-                chisq = temp;
-                s_last = misc[M_SAREA];
-                if (temp < ochisq) {
-                    alamda = alamda / P.alamda_incr;
-                    double* t1 = alpha;
-                    alpha = covar;
-                    covar = t1;
-                    t1 = beta;
-                    beta = da;
-                    da = t1;
-                    for (int i = tid; i < ma; i += kThreads) cg[i] = atry[i];
-                    cur0 = misc[M_CHK0];
-                    cur1 = misc[M_CHK0 + 1];
-                    cur2 = misc[M_CHK0 + 2];
-                    s_cur = misc[M_SAREA];
-                } else {
-                    alamda = P.alamda_incr * alamda;
-                    chisq = ochisq;
-                }
-            } else {
-                if (status == 0) status = err;
-                // The reference leaves its global Chisq untouched here; at the
-                // first step that is the previous fit's value.  A fit on its own
-                // uses its first chi2 instead.
-                if (niter == 0) chisq = ochisq;
-            }
-            niter++;
-            if ((niter == 1) || (chisq < ochisq)) {
-                ochisq = chisq;
-                chk0 = cur0;
-                chk1 = cur1;
-                chk2 = cur2;
-                s_last = s_cur;
-                rchisq = chisq - (chk0 * chk0 + chk1 * chk1 + chk2 * chk2) * (P.conw_r * P.conw_r);
-            }
-            dev_new = sqrt(rchisq / P.ndata_m3);
-            if (dev_old - dev_new > 1e-10) {
-                iter_diff = dev_old - dev_new;
-                dev_old = dev_new;
-            }
-            __syncthreads();
-        }
-        if (tid == 0) {
-            FitOut o;
-            o.dev = dev_new;
-            o.dark = sqrt(chk0 * chk0 + chk1 * chk1 + chk2 * chk2);
-            o.totarea = s_last;
-            o.prd = 2 * kPiD / cg[C + 2];
-            o.la = (180 / kPiD) * cg[C + 1];
-            o.be = 90 - (180 / kPiD) * cg[C];
-            o.chisq = chisq;
-            o.niter = niter;
-            o.status = status;
-            Bt.out[w] = o;
-        }
-    }
-}
-
-// Single evaluation for the diagnostic API (ps_mrqcof / ps_model).
-template <int NCB>
-__global__ void __launch_bounds__(kThreads, 1) eval_kernel(const DevProblem* __restrict__ Pp, EvalOut E) {
-    extern __shared__ __align__(16) double sm[];
-    const DevProblem& P = *Pp;
-    const Layout L = make_layout(P);
-    const int tid = threadIdx.x;
-    double* cg = sm + L.cg;
-    double* Jt = E.scratch;
-    double* yt = Jt + (size_t)P.ma * P.npad;
-    entry_map(P.mfit, (int*)(sm + L.ent));
-    for (int i = tid; i < P.ma; i += kThreads) cg[i] = E.a[i];
-    __syncthreads();
-    evaluate<NCB>(Pp, sm, cg, sm + L.alpha, sm + L.beta, Jt, yt);
-    for (int i = tid; i < P.mfit * P.mfit; i += kThreads) E.alpha[i] = sm[L.alpha + i];
-    for (int i = tid; i < P.mfit; i += kThreads) E.beta[i] = sm[L.beta + i];
-    if (tid == 0) E.chisq[0] = sm[L.misc + M_CHISQ];
-    for (int idx = tid; idx < P.n_rows * P.ma; idx += kThreads) {
-        const int r = idx / P.ma, l = idx - r * P.ma;
-        E.J[idx] = Jt[(size_t)l * P.npad + r];
-    }
-    for (int r = tid; r < P.n_rows; r += kThreads) E.y[r] = yt[r];
-}
 
 // Best-of-poles record per trial period (period_search_BOINC.cpp:811-931).
 struct RecordOut {
@@ -562,79 +74,51 @@ __global__ void period_reduce_kernel(const FitOut* fits, int n_periods, double n
     rec[n] = r;
 }
 
-template <int NCB>
-cudaError_t launch_fits_t(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s) {
-    const Layout L = make_layout(P);
-    cudaError_t e = cudaFuncSetAttribute(fit_kernel<NCB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
-    if (e != cudaSuccess) return e;
-    fit_kernel<NCB><<<grid, kThreads, L.bytes, s>>>(dP, B);
-    return cudaGetLastError();
-}
-
-template <int NCB>
-cudaError_t launch_eval_t(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s) {
-    const Layout L = make_layout(P);
-    cudaError_t e = cudaFuncSetAttribute(eval_kernel<NCB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes);
-    if (e != cudaSuccess) return e;
-    eval_kernel<NCB><<<1, kThreads, L.bytes, s>>>(dP, E);
-    return cudaGetLastError();
-}
-
-template <int NCB>
-int max_blocks_t(const DevProblem& P) {
-    const Layout L = make_layout(P);
-    if (cudaFuncSetAttribute(fit_kernel<NCB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.bytes) != cudaSuccess)
-        return 0;
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fit_kernel<NCB>, kThreads, L.bytes) != cudaSuccess) return 0;
-    return nb;
-}
-
 }  // namespace
 
-size_t fp64_smem_bytes(const DevProblem& P) { return make_layout(P).bytes; }
+size_t fp64_smem_bytes(const DevProblem& P) { return fitimpl::make_layout(P).bytes; }
 
 int fp64_max_blocks_per_sm(const DevProblem& P, int* threads) {
-    if (threads) *threads = kThreads;
+    if (threads) *threads = fitcommon::kThreads;
     switch (P.NCB) {
-        case 8: return max_blocks_t<8>(P);
-        case 16: return max_blocks_t<16>(P);
-        case 24: return max_blocks_t<24>(P);
-        case 32: return max_blocks_t<32>(P);
-        case 40: return max_blocks_t<40>(P);
-        case 48: return max_blocks_t<48>(P);
-        case 56: return max_blocks_t<56>(P);
-        case 64: return max_blocks_t<64>(P);
+        case 8: return fitimpl::max_blocks_t<8, false>(P);
+        case 16: return fitimpl::max_blocks_t<16, false>(P);
+        case 24: return fitimpl::max_blocks_t<24, false>(P);
+        case 32: return fitimpl::max_blocks_t<32, false>(P);
+        case 40: return fitimpl::max_blocks_t<40, false>(P);
+        case 48: return fitimpl::max_blocks_t<48, false>(P);
+        case 56: return fitimpl::max_blocks_t<56, false>(P);
+        case 64: return fitimpl::max_blocks_t<64, false>(P);
         default: return 0;
     }
 }
 
 cudaError_t launch_fp64_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s) {
-    if (P.nq <= 0 || P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 > kMaxEpt * kThreads) return cudaErrorInvalidValue;
+    if (P.nq <= 0 || P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 > fitimpl::kMaxEpt * fitcommon::kThreads) return cudaErrorInvalidValue;
     switch (P.NCB) {
-        case 8: return launch_fits_t<8>(P, dP, B, grid, s);
-        case 16: return launch_fits_t<16>(P, dP, B, grid, s);
-        case 24: return launch_fits_t<24>(P, dP, B, grid, s);
-        case 32: return launch_fits_t<32>(P, dP, B, grid, s);
-        case 40: return launch_fits_t<40>(P, dP, B, grid, s);
-        case 48: return launch_fits_t<48>(P, dP, B, grid, s);
-        case 56: return launch_fits_t<56>(P, dP, B, grid, s);
-        case 64: return launch_fits_t<64>(P, dP, B, grid, s);
+        case 8: return fitimpl::launch_fits_t<8, false>(P, dP, B, grid, s);
+        case 16: return fitimpl::launch_fits_t<16, false>(P, dP, B, grid, s);
+        case 24: return fitimpl::launch_fits_t<24, false>(P, dP, B, grid, s);
+        case 32: return fitimpl::launch_fits_t<32, false>(P, dP, B, grid, s);
+        case 40: return fitimpl::launch_fits_t<40, false>(P, dP, B, grid, s);
+        case 48: return fitimpl::launch_fits_t<48, false>(P, dP, B, grid, s);
+        case 56: return fitimpl::launch_fits_t<56, false>(P, dP, B, grid, s);
+        case 64: return fitimpl::launch_fits_t<64, false>(P, dP, B, grid, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_fp64_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s) {
-    if (P.nq <= 0 || P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 > kMaxEpt * kThreads) return cudaErrorInvalidValue;
+    if (P.nq <= 0 || P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 > fitimpl::kMaxEpt * fitcommon::kThreads) return cudaErrorInvalidValue;
     switch (P.NCB) {
-        case 8: return launch_eval_t<8>(P, dP, E, s);
-        case 16: return launch_eval_t<16>(P, dP, E, s);
-        case 24: return launch_eval_t<24>(P, dP, E, s);
-        case 32: return launch_eval_t<32>(P, dP, E, s);
-        case 40: return launch_eval_t<40>(P, dP, E, s);
-        case 48: return launch_eval_t<48>(P, dP, E, s);
-        case 56: return launch_eval_t<56>(P, dP, E, s);
-        case 64: return launch_eval_t<64>(P, dP, E, s);
+        case 8: return fitimpl::launch_eval_t<8, false>(P, dP, E, s);
+        case 16: return fitimpl::launch_eval_t<16, false>(P, dP, E, s);
+        case 24: return fitimpl::launch_eval_t<24, false>(P, dP, E, s);
+        case 32: return fitimpl::launch_eval_t<32, false>(P, dP, E, s);
+        case 40: return fitimpl::launch_eval_t<40, false>(P, dP, E, s);
+        case 48: return fitimpl::launch_eval_t<48, false>(P, dP, E, s);
+        case 56: return fitimpl::launch_eval_t<56, false>(P, dP, E, s);
+        case 64: return fitimpl::launch_eval_t<64, false>(P, dP, E, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -13,6 +13,11 @@ oracle/Makefile (`make -C oracle ref`):
   fma_out.full  the same source rebuilt with FMA contraction; a period whose
                 chi2 differs between the two builds is "chaotic" (its LM
                 trajectory amplifies last-ulp differences)
+  var_*.full    the oracle restatement (bit-identical to the reference build)
+                rebuilt with other last-ulp perturbations -- pow(x,2) -> x*x
+                (sq), FMA contraction (fma), both (fmasq) -- at the
+                reference's conw_r; together with fma_out.full they define the
+                chaotic periods: those that any of these perturbations moves
 
 Long scans are split across host cores the way the reference allows it:
 each slice keeps P_start (so the convexity pre-pass sees the same first ten
@@ -112,6 +117,39 @@ def run_reference(exe, text, n_periods, workers):
     return "".join(o[0] for o in outs), "".join(o[1] for o in outs)
 
 
+def _run_variant_slice(exe, text, n_from, n_to, conw_r):
+    d = tempfile.mkdtemp(prefix="psvar")
+    try:
+        open(os.path.join(d, "period_search_in"), "w").write(text)
+        subprocess.run([exe, d, str(n_from), str(n_to), "%.17g" % conw_r], check=True, stdout=subprocess.DEVNULL)
+        return open(os.path.join(d, "period_search_out.full")).read()
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def make_variants(name, workers):
+    import math
+
+    import pso
+
+    d = os.path.join(HERE, name)
+    text = open(os.path.join(d, "period_search_in")).read()
+    ref = pso.read_full(os.path.join(d, "ref_out.full"))
+    o = pso.Oracle(os.path.join(d, "period_search_in"))
+    k = round(math.log2(ref["dark_pct"][0] / (o.conw_r * o.escl * o.escl)))
+    conw_r = o.conw_r * 2.0**k
+    n = len(ref)
+    per = max(1, -(-n // workers))
+    slices = [(a, min(a + per - 1, n)) for a in range(1, n + 1, per)]
+    for var in ("sq", "fma", "fmasq"):
+        exe = os.path.join(REPO, "oracle", "ps_oracle_" + var)
+        with cf.ProcessPoolExecutor(max_workers=workers) as ex:
+            outs = list(ex.map(_run_variant_slice, [exe] * len(slices), [text] * len(slices),
+                               [s[0] for s in slices], [s[1] for s in slices], [conw_r] * len(slices)))
+        open(os.path.join(d, "var_%s.full" % var), "w").write("".join(outs))
+    print(name, "variants written", flush=True)
+
+
 def make_workload(name, text, n_periods, workers):
     d = os.path.join(HERE, name)
     os.makedirs(d, exist_ok=True)
@@ -202,7 +240,7 @@ def make_unit():
 def main(names):
     from periodsearch_b200 import synth
 
-    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "all", "ref"], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "all", "variants", "ref"], check=True)
     workers = os.cpu_count() or 4
     if "unit" in names:
         make_unit()
@@ -216,7 +254,10 @@ def main(names):
         if name in names:
             w = fn()
             make_workload(name, w.text, w.n_periods, workers if w.n_periods > 20 else 1)
+    for name in ("tiny", "tiny_rel", "c1", "shipped"):
+        if name in names or "variants" in names:
+            make_variants(name, workers)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["unit", "shipped", "tiny", "tiny_rel", "c1"])
+    main(sys.argv[1:] or ["unit", "shipped", "tiny", "tiny_rel", "c1", "variants"])

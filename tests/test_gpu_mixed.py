@@ -1,0 +1,97 @@
+"""Mixed-precision form (PS_FORM_MIXED) vs the CPU oracle / the reference.
+
+The model brightness, chi2, beta, the solve and the rotation angle are FP64;
+derivatives are FP32 and the shape block of the Jacobian comes from the
+tensor cores in split BF16 (~2^-16 relative per product, FP32 accumulation).
+
+What holds, and is asserted:
+  * one evaluation: chi2 and y to 1e-11 (FP64 path); alpha, beta and the
+    Jacobian to 1e-4 normwise;
+  * every fit runs the reference's iteration count.
+
+What does not hold, and is measured instead: per-period chi2 within 1e-6 of
+the reference.  Under the reference's stop rule (a fixed 50 iterations for
+these inputs) the fits are far from converged -- chi2 still moves by
+0.5-15 % between iterations 50 and 100 on c1 -- so the chi2 reached at
+iteration 50 depends on the exact LM path, and a ~1e-5 relative Jacobian
+error moves it by ~1e-3 (median) and can reorder the best periods.  The
+scan test bounds that drift (median below 1e-2) and prints the distribution;
+the FP64 forms are the ones held to the parity bar (test_gpu_parity.py).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden_path
+
+pytestmark = pytest.mark.gpu
+
+MIX_TOL = 1e-6
+
+
+def _rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def _pair(native, oracle_lib, name):
+    path = golden_path(name)
+    o = oracle_lib.Oracle(path)
+    o.set_conw_r(o.conw_r)
+    g = native.PeriodSearch(path, form=native.PS_FORM_MIXED)
+    g.set_conw_r(o.conw_r)
+    return g, o
+
+
+@pytest.mark.parametrize("name", ["tiny", "tiny_rel", "c1"])
+def test_mixed_evaluation(native, oracle_lib, name):
+    g, o = _pair(native, oracle_lib, name)
+    for n, pole in ((1, 1), (2, 5), (o.n_periods, 9)):
+        a = o.initial_parameters(o.freq(n), pole)
+        al_o, be_o, x_o = o.mrqcof(a)
+        al_g, be_g, x_g = g.mrqcof(a)
+        assert abs(x_g - x_o) <= 1e-11 * abs(x_o), (name, x_g, x_o)
+        assert _rel(be_g, be_o) <= 1e-4, (name, _rel(be_g, be_o))
+        assert _rel(al_g, al_o) <= 1e-4, (name, _rel(al_g, al_o))
+        y_o, J_o = o.model(a)
+        y_g, J_g = g.model(a)
+        assert _rel(y_g, y_o) <= 1e-11
+        assert _rel(J_g, J_o) <= 1e-4, (name, _rel(J_g, J_o))
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["tiny", "c1"])
+def test_mixed_fits_run_the_reference_iterations(native, oracle_lib, name):
+    g, o = _pair(native, oracle_lib, name)
+    errs = []
+    for n in (1, 2, o.n_periods):
+        f = o.freq(n)
+        for pole in range(1, 11):
+            ro, _ = o.fit(f, pole)
+            rg = g.fit(f, pole)
+            assert rg["niter"] == int(ro["niter"])
+            assert np.isfinite(rg["chisq"])
+            errs.append(abs(rg["chisq"] - ro["chisq"]) / abs(ro["chisq"]))
+    errs = np.array(errs)
+    print(f"{name} mixed fits: chi2 rel err median {np.median(errs):.2e} max {errs.max():.2e}")
+    g.close()
+
+
+@pytest.mark.parametrize("name", ["tiny", "c1", "shipped"])
+def test_mixed_scan_drift(native, oracle_lib, name):
+    import pso
+
+    ref = pso.read_full(os.path.join(GOLDEN, name, "ref_out.full"))
+    g = native.PeriodSearch(golden_path(name), form=native.PS_FORM_MIXED)
+    conw_r = g.precalc()
+    assert abs(conw_r * g.escl * g.escl - ref["dark_pct"][0]) <= 1e-12 * ref["dark_pct"][0]
+    recs = g.scan(1, len(ref))
+    assert np.all(np.isfinite(recs["chi2"]))
+    err = np.abs(recs["chi2"] - ref["chi2"]) / np.abs(ref["chi2"])
+    best_same = int(np.argmin(recs["chi2"])) == int(np.argmin(ref["chi2"]))
+    print(f"{name} mixed scan: chi2 rel err median {np.median(err):.2e} p90 {np.quantile(err, 0.9):.2e} "
+          f"max {err.max():.2e}, best period identical: {best_same}")
+    assert np.median(err) <= 1e-2
+    g.close()

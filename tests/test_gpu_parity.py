@@ -1,12 +1,17 @@
 """FP64 GPU form vs the CPU oracle, through the C ABI (libps_b200.so).
 
-Tolerances (FP64 form): one model evaluation (the reference's mrqcof) agrees
+Both FP64 forms are held to the same bars: PS_FORM_FP64 (the reference's
+operation order) and PS_FORM_FAST (rearranged, fused; rounding-level
+differences).
+
+Tolerances: one model evaluation (the reference's mrqcof) agrees
 to 1e-11 relative (normwise for alpha, beta and the Jacobian rows) -- the
 only differences are last-ulp libm results (exp, sin, cos, pow(x,2) = x*x);
 whole fits and scans agree to 1e-9 relative in chi2/rms, except on periods
 whose LM trajectory is chaotic, i.e. where the reference itself changes by
-more than that when rebuilt with FMA contraction; there the GPU value must
-lie within the reference-vs-reference spread.  Dark-facet percentages agree
+more than that under a last-ulp perturbation (rebuilt with FMA contraction,
+or the bit-identical restatement rebuilt with FMA and/or x*x for pow(x,2));
+there the GPU value must lie within ten times the largest such spread.  Dark-facet percentages agree
 to 1e-6 (absolute) and the best-period ranking is identical.
 """
 import os
@@ -29,19 +34,27 @@ def _rel(a, b):
     return float(np.linalg.norm((a - b).ravel()) / den)
 
 
-def _pair(native, oracle_lib, name):
+FORMS = ["fp64", "fast"]
+
+
+def _form(native, form):
+    return {"fp64": native.PS_FORM_FP64, "fast": native.PS_FORM_FAST}[form]
+
+
+def _pair(native, oracle_lib, name, form="fp64"):
     path = golden_path(name)
     o = oracle_lib.Oracle(path)
     conw_r = o.conw_r
     o.set_conw_r(conw_r)
-    g = native.PeriodSearch(path)
+    g = native.PeriodSearch(path, form=_form(native, form))
     g.set_conw_r(conw_r)
     return g, o
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("name", ["tiny", "tiny_rel", "c1"])
-def test_mrqcof_matches_oracle(native, oracle_lib, name):
-    g, o = _pair(native, oracle_lib, name)
+def test_mrqcof_matches_oracle(native, oracle_lib, name, form):
+    g, o = _pair(native, oracle_lib, name, form)
     rng = np.random.default_rng(5)
     for n, pole in ((1, 1), (2, 5), (o.n_periods, 9)):
         a = o.initial_parameters(o.freq(n), pole)
@@ -63,9 +76,10 @@ def test_mrqcof_matches_oracle(native, oracle_lib, name):
     g.close()
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("name", ["tiny", "tiny_rel"])
-def test_fits_match_oracle(native, oracle_lib, name):
-    g, o = _pair(native, oracle_lib, name)
+def test_fits_match_oracle(native, oracle_lib, name, form):
+    g, o = _pair(native, oracle_lib, name, form)
     worst = 0.0
     for n in range(1, o.n_periods + 1):
         f = o.freq(n)
@@ -93,13 +107,25 @@ def _read_full(path):
     return pso.read_full(path)
 
 
-def check_records(gpu, ref, fma, label):
+def perturbation_spread(name, ref):
+    """Largest relative chi2 change per period among last-ulp perturbations of
+    the reference: its FMA rebuild and the restatement's perturbed builds
+    (tests/golden/make_golden.py)."""
+    spread = np.zeros(len(ref))
+    for f in ("fma_out.full", "var_sq.full", "var_fma.full", "var_fmasq.full"):
+        path = os.path.join(GOLDEN, name, f)
+        if os.path.exists(path):
+            x = _read_full(path)
+            spread = np.maximum(spread, np.abs(x["chi2"] - ref["chi2"]) / np.abs(ref["chi2"]))
+    return spread
+
+
+def check_records(gpu, ref, spread, label):
     """Per-period parity with the chaotic-period triage, plus the ranking."""
     assert gpu.shape == ref.shape
     n = len(ref)
-    chaotic = np.abs(fma["chi2"] - ref["chi2"]) > FIT_TOL * np.abs(ref["chi2"])
+    chaotic = spread > FIT_TOL
     err = np.abs(gpu["chi2"] - ref["chi2"]) / np.abs(ref["chi2"])
-    spread = np.abs(fma["chi2"] - ref["chi2"]) / np.abs(ref["chi2"])
     ok = (err <= FIT_TOL) | (chaotic & (err <= np.maximum(spread, FIT_TOL) * 10))
     bad = np.nonzero(~ok)[0]
     assert len(bad) == 0, (label, [(int(i) + 1, float(err[i]), float(spread[i])) for i in bad[:10]])
@@ -117,17 +143,19 @@ def check_records(gpu, ref, fma, label):
     return int(chaotic.sum()), float(err.max())
 
 
+@pytest.mark.parametrize("form", FORMS)
 @pytest.mark.parametrize("name", ["tiny", "tiny_rel", "c1", "shipped"])
-def test_scan_matches_reference(native, oracle_lib, name):
+def test_scan_matches_reference(native, oracle_lib, name, form):
     ref_full = os.path.join(GOLDEN, name, "ref_out.full")
     if not os.path.exists(ref_full):
         pytest.skip("fixture not generated")
     ref = _read_full(ref_full)
-    fma = _read_full(os.path.join(GOLDEN, name, "fma_out.full"))
-    g = native.PeriodSearch(golden_path(name))
+    spread = perturbation_spread(name, ref)
+    g = native.PeriodSearch(golden_path(name), form=_form(native, form))
     conw_r = g.precalc()
     recs = g.scan(1, len(ref))
     # the first record's 4th column is conw_r * escl^2 in the reference output
     assert abs(conw_r * g.escl * g.escl - ref["dark_pct"][0]) <= 1e-12 * ref["dark_pct"][0]
-    check_records(recs, ref, fma, name)
+    n_chaotic, worst = check_records(recs, ref, spread, name)
+    print(f"{name} {form}: {n_chaotic} chaotic periods of {len(ref)}, worst chi2 rel err {worst:.3e}")
     g.close()
