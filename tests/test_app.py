@@ -1,0 +1,77 @@
+"""The drop-in executable periodsearch_b200/period_search_b200: the
+reference's file contract (period_search_in -> period_search_out, in the
+reference's 6-column format), checkpoint/resume through period_search_state
+(the CUDA application's "nlines newConw conw_r" form and the CPU
+application's bare "nlines", which re-runs the convexity pre-pass), and the
+reference's exit codes."""
+import os
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import REPO, golden_path
+
+EXE = os.path.join(REPO, "periodsearch_b200", "period_search_b200")
+
+
+def _lines_close(got, want):
+    """Printed records agree: same columns, numbers equal to the printed
+    precision except in the last printed digit (rounding of values that
+    differ by ~1e-9 relative can straddle a printed digit)."""
+    assert len(got) == len(want)
+    for g, w in zip(got, want):
+        gv = [float(x) for x in g.split()]
+        wv = [float(x) for x in w.split()]
+        assert len(gv) == len(wv) == 6
+        for a, b, q in zip(gv, wv, (1e-8, 1e-6, 1e-6, 0.1, 1.0, 1.0)):
+            assert abs(a - b) <= q * 1.01, (g, w)
+
+
+def _run(d, *args):
+    return subprocess.run([EXE, "--dir", str(d), *args], capture_output=True, text=True, timeout=600)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["tiny", "c1"])
+def test_executable_matches_reference_output(native, tmp_path, name):
+    shutil.copy(golden_path(name), tmp_path / "period_search_in")
+    r = _run(tmp_path)
+    assert r.returncode == 0, r.stderr
+    got = (tmp_path / "period_search_out").read_text().splitlines()
+    want = open(golden_path(name, "ref_out.txt")).read().splitlines()
+    _lines_close(got, want)
+    n = len(want)
+    assert (tmp_path / "period_search_state").read_text().split()[0] == str(n)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("state_form", ["cuda", "cpu"])
+def test_executable_resumes_from_checkpoint(native, tmp_path, state_form):
+    shutil.copy(golden_path("tiny"), tmp_path / "period_search_in")
+    full = tmp_path / "full"
+    full.mkdir()
+    shutil.copy(golden_path("tiny"), full / "period_search_in")
+    assert _run(full).returncode == 0
+    whole = (full / "period_search_out").read_text().splitlines(True)
+    state = (full / "period_search_state").read_text().split()
+    # interrupted after two periods
+    (tmp_path / "period_search_out").write_text("".join(whole[:2]))
+    if state_form == "cuda":
+        (tmp_path / "period_search_state").write_text("2 1 %s" % state[2])
+    else:
+        (tmp_path / "period_search_state").write_text("2")
+    r = _run(tmp_path, "--chunk", "1")
+    assert r.returncode == 0, r.stderr
+    assert (tmp_path / "period_search_out").read_text().splitlines(True) == whole
+
+
+def test_executable_exit_codes(native, tmp_path):
+    if not os.path.exists(EXE):
+        pytest.skip("executable not built")
+    r = _run(tmp_path)  # no input file
+    assert r.returncode == 255  # exit(-1)
+    (tmp_path / "period_search_in").write_text("90 0.5 100 1\n0\n")
+    r = _run(tmp_path)
+    assert r.returncode == 2
