@@ -141,6 +141,27 @@ int ps_scan_device(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, void* st
  * make it before any stream capture.  FP64 form only. */
 int ps_scan_device_noalloc(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, void* stream);
 
+/* Batched scans: many asteroids in one persistent launch, each fit pulling
+ * from one device work queue (uneven point counts and per-fit LM
+ * convergence do not stall one another), the steady state replayed from a
+ * CUDA graph.  The reference runs one asteroid per process and, in its CUDA
+ * port, one thread block per trial period of that asteroid
+ * (period_search_cuda/period_search/start_CUDA.cu:654-776); a batch spans
+ * asteroids.  The contexts must share the device, the form (PS_FORM_FP64 or
+ * PS_FORM_FAST) and lmax, mmax, nrows, and have conw_r settled
+ * (ps_precalc / ps_set_conw_r).  The batch borrows the contexts' tables:
+ * close the batch before its contexts. */
+typedef struct ps_batch ps_batch;
+int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out);
+/* Scan periods n_from[a]..n_to[a] of every asteroid a; records are
+ * concatenated in asteroid order (host memory). */
+int ps_batch_scan(ps_batch* batch, const int* n_from, const int* n_to, ps_record* out);
+/* Same into device memory, ordered before later work on `stream`. */
+int ps_batch_scan_device(ps_batch* batch, const int* n_from, const int* n_to, ps_record* d_out, void* stream);
+/* SM clock cycles spent on each asteroid's fits in the last scan. */
+int ps_batch_fit_cycles(ps_batch* batch, long long* cycles);
+void ps_batch_close(ps_batch* batch);
+
 /* One LM fit at trial frequency freq [1/day] from initial pole m (1..10)
  * (period_search_BOINC.cpp:817-920).  cg_out (may be NULL) receives the
  * final parameter vector (ma values). */

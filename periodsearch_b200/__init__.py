@@ -20,6 +20,7 @@ import numpy as np
 
 __all__ = [
     "PeriodSearch",
+    "PeriodSearchBatch",
     "PeriodSearchError",
     "RECORD_DTYPE",
     "FIT_DTYPE",
@@ -113,6 +114,7 @@ EXPORTS = (
     "ps_open_file", "ps_open", "ps_close", "ps_precalc", "ps_set_conw_r", "ps_n_periods", "ps_scan",
     "ps_scan_device", "ps_fit", "ps_mrqcof", "ps_model", "ps_info", "ps_get_array", "ps_open_host_only",
     "ps_format_record", "ps_last_error", "ps_kernel_launches", "ps_scan_device_noalloc",
+    "ps_batch_open", "ps_batch_scan", "ps_batch_scan_device", "ps_batch_fit_cycles", "ps_batch_close",
 )
 
 
@@ -144,6 +146,11 @@ def load_library(path: str | None = None):
         "ps_get_array": (ctypes.c_int, [vp, ctypes.c_char_p, _D]),
         "ps_format_record": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_double, ctypes.c_char_p, ctypes.c_int]),
         "ps_last_error": (ctypes.c_char_p, []),
+        "ps_batch_open": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]),
+        "ps_batch_scan": (ctypes.c_int, [vp, _I, _I, vp]),
+        "ps_batch_scan_device": (ctypes.c_int, [vp, _I, _I, vp, vp]),
+        "ps_batch_fit_cycles": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),
+        "ps_batch_close": (None, [vp]),
         "ps_kernel_launches": (ctypes.c_longlong, []),
     }
     for name, (res, args) in sig.items():
@@ -254,6 +261,55 @@ class PeriodSearch:
         if n < 0:
             raise PeriodSearchError(PS_ERR_ARG, "unknown array " + name)
         return out[:n]
+
+
+class PeriodSearchBatch:
+    """Several asteroids (PeriodSearch contexts with the same lmax, mmax,
+    nrows, device and FP64 form) scanned in one persistent launch."""
+
+    def __init__(self, contexts):
+        self._lib = load_library()
+        self._ctx = list(contexts)
+        arr = (ctypes.c_void_p * len(self._ctx))(*[c._h.value for c in self._ctx])
+        self._h = ctypes.c_void_p()
+        _check(self._lib.ps_batch_open(arr, len(self._ctx), ctypes.byref(self._h)))
+
+    def _ranges(self, n_from, n_to):
+        a = np.ascontiguousarray(n_from, dtype=np.int32)
+        b = np.ascontiguousarray(n_to, dtype=np.int32)
+        if a.shape != (len(self._ctx),) or b.shape != a.shape:
+            raise PeriodSearchError(PS_ERR_ARG, "one period range per asteroid")
+        return a, b
+
+    def scan(self, n_from, n_to):
+        """Records per asteroid (list of arrays)."""
+        a, b = self._ranges(n_from, n_to)
+        counts = (b - a + 1).astype(np.int64)
+        out = np.zeros(int(counts.sum()), dtype=RECORD_DTYPE)
+        _check(self._lib.ps_batch_scan(self._h, a.ctypes.data_as(_I), b.ctypes.data_as(_I),
+                                       out.ctypes.data_as(ctypes.c_void_p)))
+        return np.split(out, np.cumsum(counts)[:-1])
+
+    def scan_device(self, n_from, n_to, d_out_ptr: int, stream_ptr: int = 0):
+        a, b = self._ranges(n_from, n_to)
+        _check(self._lib.ps_batch_scan_device(self._h, a.ctypes.data_as(_I), b.ctypes.data_as(_I),
+                                              ctypes.c_void_p(d_out_ptr), ctypes.c_void_p(stream_ptr or None)))
+
+    def fit_cycles(self) -> np.ndarray:
+        c = np.zeros(len(self._ctx), dtype=np.int64)
+        _check(self._lib.ps_batch_fit_cycles(self._h, c.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
+        return c
+
+    def close(self):
+        if self._h:
+            self._lib.ps_batch_close(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _make_desc(d: dict):

@@ -44,7 +44,9 @@ struct DevProblem {
 struct FitOut {
     double dev, dark, totarea, prd, la, be, chisq;
     int niter, status;
+    long long cycles;  // SM clock cycles the fit took (per-asteroid timing)
 };
+static_assert(sizeof(FitOut) == 72, "the C ABI documents 72 bytes per fit");
 
 // A batch of fits: fit w is trial period n_from + w / 10, pole w % 10 + 1,
 // unless `freq_override` > 0 (single-fit API), then the only fit uses it.
@@ -57,6 +59,15 @@ struct FitBatch {
     FitOut* out;             // [n_fits]
     double* scratch;         // per resident CTA: J^T (ma x npad) + y (npad)
     long long scratch_stride;
+    // Several asteroids in one launch (the problem pointer is then an array):
+    // fits [ast_fit_off[a], ast_fit_off[a+1]) belong to asteroid a, ten per
+    // trial period from period ast_n_from[a].  n_ast == 0: one asteroid.
+    // n_fits_dev, if set, holds the fit count (kept in device memory so that a
+    // captured CUDA graph can be replayed for batches of any size).
+    int n_ast;
+    const int* ast_fit_off;
+    const int* ast_n_from;
+    const int* n_fits_dev;
 };
 
 // Diagnostics of one evaluation (ps_mrqcof / ps_model): J, y, alpha, beta.
@@ -88,6 +99,12 @@ int mixed_max_blocks_per_sm(const DevProblem& P, int* threads);
 cudaError_t launch_mixed_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s);
 cudaError_t launch_mixed_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s);
 inline long long mixed_scratch_doubles(const DevProblem& P) { return ((long long)P.ma * P.npad + 1) / 2 + P.npad; }
+
+// Best-of-poles records for a batch: periods [per_off[a], per_off[a+1]) of
+// the concatenated records belong to asteroid a (ndata_m3[a]); the period
+// count is read from *n_periods_dev.
+cudaError_t launch_period_reduce_batch(const FitOut* fits, const int* n_periods_dev, int max_periods, int n_ast,
+                                       const int* per_off, const double* ndata_m3, void* records, cudaStream_t s);
 
 cudaError_t launch_period_reduce(const FitOut* fits, int n_periods, double ndata_m3, int prepass,
                                  void* records /* ps_record[n_periods] */, cudaStream_t s);

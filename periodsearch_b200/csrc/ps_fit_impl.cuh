@@ -379,34 +379,61 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
 }
 
 template <int NCB, bool kFast>
-__global__ void __launch_bounds__(kThreads, 1) fit_kernel(const DevProblem* __restrict__ Pp, FitBatch Bt) {
+__global__ void __launch_bounds__(kThreads, 1) fit_kernel(const DevProblem* __restrict__ Parr, FitBatch Bt) {
     extern __shared__ __align__(16) double sm[];
-    const DevProblem& P = *Pp;
-    const Layout L = make_layout(P);
+    __shared__ int s_work, s_ast;
     const int tid = threadIdx.x;
-    const int C = P.C, ma = P.ma, mfit = P.mfit;
-    double* cg = sm + L.cg;
-    double* atry = sm + L.atry;
-    double* misc = sm + L.misc;
-    int* ipiv = (int*)(sm + L.ipiv);
-    double* Jt = Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride;
-    double* yt = Jt + (size_t)ma * P.npad;
-    entry_map(mfit, (int*)(sm + L.ent));
-
+    int cur_mfit = -1, cur_ent = -1;
     for (;;) {
         __syncthreads();
-        if (tid == 0) misc[M_WORK] = (double)atomicAdd(Bt.queue, 1);
+        if (tid == 0) {
+            const int nf = Bt.n_fits_dev ? *Bt.n_fits_dev : Bt.n_fits;
+            int w = atomicAdd(Bt.queue, 1);
+            int a = 0;
+            if (w >= nf) {
+                w = -1;
+            } else if (Bt.n_ast > 1) {
+                int lo = 0, hi = Bt.n_ast - 1;  // last a with ast_fit_off[a] <= w
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (Bt.ast_fit_off[mid] <= w)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                a = lo;
+            }
+            s_work = w;
+            s_ast = a;
+        }
         __syncthreads();
-        const int w = (int)misc[M_WORK];
-        if (w >= Bt.n_fits) break;
+        const int w = s_work;
+        if (w < 0) break;
+        const DevProblem* Pp = Parr + s_ast;
+        const DevProblem& P = *Pp;
+        const Layout L = make_layout(P);
+        const int C = P.C, ma = P.ma, mfit = P.mfit;
+        double* cg = sm + L.cg;
+        double* atry = sm + L.atry;
+        double* misc = sm + L.misc;
+        int* ipiv = (int*)(sm + L.ipiv);
+        double* Jt = Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride;
+        double* yt = Jt + (size_t)ma * P.npad;
+        if (mfit != cur_mfit || L.ent != cur_ent) {
+            entry_map(mfit, (int*)(sm + L.ent));
+            cur_mfit = mfit;
+            cur_ent = L.ent;
+        }
+        const long long t_start = clock64();
         double freq;
         int pole;
         if (Bt.pole_override) {
             freq = Bt.freq_override;
             pole = Bt.pole_override;
         } else {
-            const int n = Bt.n_from + w / 10;
-            pole = w % 10 + 1;
+            const int local = Bt.n_ast > 1 ? w - Bt.ast_fit_off[s_ast] : w;
+            const int n = (Bt.n_ast > 1 ? Bt.ast_n_from[s_ast] : Bt.n_from) + local / 10;
+            pole = local % 10 + 1;
             freq = P.freq_start - (n - 1) * P.freq_step;
         }
         // initial parameters, period_search_BOINC.cpp:819-844
@@ -524,6 +551,7 @@ __global__ void __launch_bounds__(kThreads, 1) fit_kernel(const DevProblem* __re
             o.chisq = chisq;
             o.niter = niter;
             o.status = status;
+            o.cycles = clock64() - t_start;
             Bt.out[w] = o;
         }
     }

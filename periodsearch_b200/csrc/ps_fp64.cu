@@ -74,7 +74,52 @@ __global__ void period_reduce_kernel(const FitOut* fits, int n_periods, double n
     rec[n] = r;
 }
 
+// Batched variant: global period g belongs to the asteroid a with
+// per_off[a] <= g < per_off[a+1].
+__global__ void period_reduce_batch_kernel(const FitOut* fits, const int* n_periods_dev, int n_ast, const int* per_off,
+                                           const double* ndata_m3, RecordOut* rec) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= *n_periods_dev) return;
+    int lo = 0, hi = n_ast - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (per_off[mid] <= g)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    double per_best = 0, dark_best = 0, la_best = 0, be_best = 0, dev_best = 1e40;
+    for (int m = 0; m < 10; m++) {
+        const FitOut& f = fits[(size_t)g * 10 + m];
+        if (f.dev < dev_best) {
+            dev_best = f.dev;
+            per_best = f.prd;
+            dark_best = f.dark / f.totarea * 100;
+            la_best = f.la;
+            be_best = f.be;
+        }
+    }
+    if (la_best < 0) la_best += 360;
+    RecordOut r;
+    r.period_h = 24 * per_best;
+    r.rms = dev_best;
+    r.chi2 = dev_best * dev_best * ndata_m3[lo];
+    r.dark_pct = dark_best;
+    r.lambda_deg = la_best;
+    r.beta_deg = be_best;
+    rec[g] = r;
+}
+
 }  // namespace
+
+cudaError_t launch_period_reduce_batch(const FitOut* fits, const int* n_periods_dev, int max_periods, int n_ast,
+                                       const int* per_off, const double* ndata_m3, void* records, cudaStream_t s) {
+    if (max_periods <= 0) return cudaSuccess;
+    const int tb = 128;
+    period_reduce_batch_kernel<<<(max_periods + tb - 1) / tb, tb, 0, s>>>(fits, n_periods_dev, n_ast, per_off, ndata_m3,
+                                                                          (RecordOut*)records);
+    return cudaGetLastError();
+}
 
 size_t fp64_smem_bytes(const DevProblem& P) { return fitimpl::make_layout(P).bytes; }
 

@@ -679,6 +679,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
             o.chisq = chisq;
             o.niter = niter;
             o.status = status;
+            o.cycles = 0;
             Bt.out[w] = o;
         }
     }

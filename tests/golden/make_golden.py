@@ -28,6 +28,8 @@ Inputs:
   shipped   the reference's own period_search/period_search_in (+ its shipped
             period_search_out as `shipped_out.txt`), first 12 periods
   tiny, tiny_rel, c1   seeded synthetic asteroids (periodsearch_b200.synth)
+  tiny_conv, c1_conv   the same with the per-fit convergence stop rule
+                       (stop_condition < 1, n_iter_min = 5)
   unit      golden arrays of the reference's unit tests
             (period_search_pure_cpu_win/UnitTest_pure_cpu_win/arrangers.cpp),
             dumped to unit.json through a small C++ harness
@@ -254,10 +256,25 @@ def main(names):
         if name in names:
             w = fn()
             make_workload(name, w.text, w.n_periods, workers if w.n_periods > 20 else 1)
-    for name in ("tiny", "tiny_rel", "c1", "shipped"):
+    # the per-fit convergence stop rule (stop_condition < 1, n_iter_min;
+    # period_search_BOINC.cpp:855-867): tiny, and the first 40 periods of c1
+    for name, fn, stop, nmin, keep in (("tiny_conv", synth._tiny, 0.0005, 5, None),
+                                       ("c1_conv", synth._c1, 0.0001, 5, 40)):
+        if name in names:
+            w = fn()
+            lines = w.text.split("\n")
+            lines[10] = "%g\t\t\t\titeration stop condition" % stop
+            lines[11] = "%d\t\t\t\tminimum number of iterations (only if the above value < 1)" % nmin
+            text = "\n".join(lines)
+            n = w.n_periods
+            if keep:
+                text = _slice_text(text, keep)
+                n = keep
+            make_workload(name, text, n, workers if n > 20 else 1)
+    for name in ("tiny", "tiny_rel", "c1", "shipped", "tiny_conv", "c1_conv"):
         if name in names or "variants" in names:
             make_variants(name, workers)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1:] or ["unit", "shipped", "tiny", "tiny_rel", "c1", "variants"])
+    main(sys.argv[1:] or ["unit", "shipped", "tiny", "tiny_rel", "c1", "tiny_conv", "c1_conv", "variants"])

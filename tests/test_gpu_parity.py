@@ -144,7 +144,7 @@ def check_records(gpu, ref, spread, label):
 
 
 @pytest.mark.parametrize("form", FORMS)
-@pytest.mark.parametrize("name", ["tiny", "tiny_rel", "c1", "shipped"])
+@pytest.mark.parametrize("name", ["tiny", "tiny_rel", "c1", "shipped", "tiny_conv", "c1_conv"])
 def test_scan_matches_reference(native, oracle_lib, name, form):
     ref_full = os.path.join(GOLDEN, name, "ref_out.full")
     if not os.path.exists(ref_full):
