@@ -156,6 +156,98 @@ def run_reference(args, path, rank):
     print(json.dumps(line), flush=True)
 
 
+def _c4_worker(args):
+    i, directory = args
+    sys.path.insert(0, REPO)
+    from periodsearch_b200 import synth
+
+    w, width = synth.c4_asteroid(i)
+    return synth.write_input(w, os.path.join(directory, "a%04d" % i)), w.n_points
+
+
+def run_c4(args, local):
+    """Uneven batch: many asteroids, point counts
+    log-uniform in 100-5000, dense/sparse mix, lmax = 6, nrows = 10,
+    per-fit convergence, all in one persistent launch replayed from a CUDA
+    graph.  A step scans `periods` consecutive trial periods of every
+    asteroid.  The convexity pre-pass is not part of the timed steps (each
+    asteroid uses conw / escl^2, the pre-pass start value)."""
+    import multiprocessing as mp
+
+    import numpy as np
+    import torch
+
+    import periodsearch_b200 as ps
+
+    workdir = tempfile.mkdtemp(prefix="psc4")
+    with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 16)) as pool:
+        made = pool.map(_c4_worker, [(i, workdir) for i in range(args.asteroids)])
+    torch.cuda.set_device(local)
+    form = {"fp64": ps.PS_FORM_FP64, "fast": ps.PS_FORM_FAST}[args.form]
+    ctxs = []
+    for p, _ in made:
+        c = ps.PeriodSearch(p, device=local, form=form)
+        c.set_conw_r(c.conw_r)
+        ctxs.append(c)
+    batch = ps.PeriodSearchBatch(ctxs)
+    P = args.c4_periods
+    n_per = np.array([c.n_periods for c in ctxs])
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    total_periods = int(len(ctxs) * P)
+    d_rec = torch.zeros(total_periods * 6, dtype=torch.float64, device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def ranges(step):
+        a = 1 + (step * P) % np.maximum(n_per - P + 1, 1)
+        return a, np.minimum(a + P - 1, n_per)
+
+    for s in range(args.warmup):
+        a, b = ranges(s)
+        batch.scan_device(a, b, d_rec.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    launches0 = ps.load_library().ps_kernel_launches()
+    times, fits, cycles = [], 0, None
+    with ClockSampler(local) as clk:
+        for s in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            a, b = ranges(args.warmup + s)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            batch.scan_device(a, b, d_rec.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1000.0)
+            fits += int(10 * (b - a + 1).sum())
+            cycles = batch.fit_cycles()
+    launches = ps.load_library().ps_kernel_launches() - launches0
+    clocks = clk.summary()
+    hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
+    per_ast = cycles / hz
+    value = fits / sum(times)
+    line = {
+        "metric": METRIC + " (uneven batch)", "value": value, "unit": "fits/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"c4 uneven batch: {len(ctxs)} asteroids, N log-uniform 100-5000 "
+                               f"(mean {np.mean([m for _, m in made]):.0f}), lmax=mmax=6, nrows=10, "
+                               f"stop_condition 1e-4 / n_iter_min 5, {P} periods x 10 poles per asteroid per step",
+                   "form": args.form, "graph": "persistent fit kernel + reduction replayed from a CUDA graph",
+                   "l2": "flushed (256 MB write) between timed steps"},
+        "per_asteroid_ms": {"p50": 1000 * float(np.percentile(per_ast, 50)),
+                            "p99": 1000 * float(np.percentile(per_ast, 99)),
+                            "what": "SM-time of one asteroid's fits in the last step (sum over its fits of "
+                                    "the fit's clock cycles / SM clock)"},
+        "gpu_launches": int(launches), "clocks": clocks,
+    }
+    batch.close()
+    for c in ctxs:
+        c.close()
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -166,6 +258,10 @@ def main():
     ap.add_argument("--form", default="fp64", choices=["fp64", "fast", "mixed"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--config", default="c2", choices=["c2", "c4"],
+                    help="c2: production sparse search (the headline); c4: uneven multi-asteroid batch")
+    ap.add_argument("--asteroids", type=int, default=512)
+    ap.add_argument("--c4-periods", type=int, default=4)
     ap.add_argument("--profile", action="store_true",
                     help="small case for ncu: 14 periods per step, no pre-pass, no e2e/cpu legs")
     args = ap.parse_args()
@@ -176,6 +272,11 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.config == "c4" and args.impl == "b200":
+        if args.form == "mixed":
+            ap.error("the batched form runs the FP64 forms")
+        run_c4(args, local)
+        return
     workdir = tempfile.mkdtemp(prefix="psbench")
     path = make_input(workdir)
 

@@ -156,7 +156,8 @@ int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out);
 /* Scan periods n_from[a]..n_to[a] of every asteroid a; records are
  * concatenated in asteroid order (host memory). */
 int ps_batch_scan(ps_batch* batch, const int* n_from, const int* n_to, ps_record* out);
-/* Same into device memory, ordered before later work on `stream`. */
+/* Same into device memory, launched on `stream` (NULL = the batch's own
+ * stream); asynchronous. */
 int ps_batch_scan_device(ps_batch* batch, const int* n_from, const int* n_to, ps_record* d_out, void* stream);
 /* SM clock cycles spent on each asteroid's fits in the last scan. */
 int ps_batch_fit_cycles(ps_batch* batch, long long* cycles);

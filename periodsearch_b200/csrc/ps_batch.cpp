@@ -40,7 +40,7 @@ struct ps_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     size_t graph_fits = 0, graph_periods = 0;
-    std::vector<long long> last_cycles;
+    cudaStream_t last = nullptr;  // stream of the last replay
 };
 
 namespace {
@@ -108,10 +108,11 @@ int capture(ps_batch* b, size_t fits, size_t periods) {
 }
 
 // Fill the control block and replay the graph; records land in d_rec.
-int run(ps_batch* b, const int* n_from, const int* n_to, size_t* periods_out) {
+int run(ps_batch* b, const int* n_from, const int* n_to, size_t* periods_out, cudaStream_t launch) {
     const int n = b->n;
     // the previous replay may still be reading the pinned control block
     PSB_BCUDA(cudaStreamSynchronize(b->stream));
+    if (b->last && b->last != b->stream) PSB_BCUDA(cudaStreamSynchronize(b->last));
     size_t fits = 0, periods = 0;
     int* h = b->h_ctl;
     for (int a = 0; a < n; a++) {
@@ -135,7 +136,8 @@ int run(ps_batch* b, const int* n_from, const int* n_to, size_t* periods_out) {
         int rc = capture(b, std::max(fits, b->graph_fits), std::max(periods, b->graph_periods));
         if (rc) return rc;
     }
-    PSB_BCUDA(cudaGraphLaunch(b->exec, b->stream));
+    PSB_BCUDA(cudaGraphLaunch(b->exec, launch));
+    b->last = launch;
     psb::count_launch();
     psb::count_launch();
     *periods_out = periods;
@@ -210,17 +212,10 @@ int ps_batch_scan_device(ps_batch* b, const int* n_from, const int* n_to, ps_rec
     if (!b || !n_from || !n_to || !d_out) return psb::set_error(PS_ERR_ARG, "null argument");
     PSB_BCUDA(cudaSetDevice(b->device));
     size_t periods = 0;
-    int rc = run(b, n_from, n_to, &periods);
+    cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+    int rc = run(b, n_from, n_to, &periods, s);
     if (rc) return rc;
-    PSB_BCUDA(cudaMemcpyAsync(d_out, b->d_rec.p, periods * sizeof(ps_record), cudaMemcpyDeviceToDevice, b->stream));
-    if (stream) {
-        // order the caller's stream after the batch's work
-        cudaEvent_t ev;
-        PSB_BCUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
-        PSB_BCUDA(cudaEventRecord(ev, b->stream));
-        PSB_BCUDA(cudaStreamWaitEvent((cudaStream_t)stream, ev, 0));
-        cudaEventDestroy(ev);
-    }
+    PSB_BCUDA(cudaMemcpyAsync(d_out, b->d_rec.p, periods * sizeof(ps_record), cudaMemcpyDeviceToDevice, s));
     return PS_OK;
 }
 
@@ -228,7 +223,7 @@ int ps_batch_scan(ps_batch* b, const int* n_from, const int* n_to, ps_record* ou
     if (!b || !n_from || !n_to || !out) return psb::set_error(PS_ERR_ARG, "null argument");
     PSB_BCUDA(cudaSetDevice(b->device));
     size_t periods = 0;
-    int rc = run(b, n_from, n_to, &periods);
+    int rc = run(b, n_from, n_to, &periods, b->stream);
     if (rc) return rc;
     PSB_BCUDA(cudaMemcpyAsync(out, b->d_rec.p, periods * sizeof(ps_record), cudaMemcpyDeviceToHost, b->stream));
     PSB_BCUDA(cudaStreamSynchronize(b->stream));
@@ -239,6 +234,7 @@ int ps_batch_fit_cycles(ps_batch* b, long long* cycles) {
     if (!b || !cycles) return psb::set_error(PS_ERR_ARG, "null argument");
     PSB_BCUDA(cudaSetDevice(b->device));
     PSB_BCUDA(cudaStreamSynchronize(b->stream));
+    if (b->last) PSB_BCUDA(cudaStreamSynchronize(b->last));
     const int n = b->n;
     const size_t fits = (size_t)b->h_ctl[0];
     std::vector<psb::FitOut> f(fits);
@@ -255,6 +251,7 @@ void ps_batch_close(ps_batch* b) {
     if (!b) return;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->last) cudaStreamSynchronize(b->last);
     release_graph(b);
     b->d_probs.release();
     b->d_ctl.release();
