@@ -24,10 +24,11 @@ using namespace fitcommon;
 constexpr int kFch = 32;     // facets per shared-memory chunk
 constexpr int kRt = 32;      // rows per alpha tile
 constexpr int kMaxEpt = 16;  // alpha/beta/chi2 entries per thread
+constexpr int kSortSeg = 1024;  // points sorted together by viewing direction
 
 // Shared-memory layout, offsets in doubles.
 struct Layout {
-    int cg, atry, alpha, covar, beta, da, g, area, dres, dave, blm, misc, red, work, ipiv, ent;
+    int cg, atry, alpha, covar, beta, da, g, area, dres, dave, blm, misc, red, perm, work, ipiv, ent;
     size_t bytes;
 };
 
@@ -54,6 +55,8 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     int tile = kRt * (P.mfit + 1) + kRt * (P.mfit + 2);
     int w = chunk > tile ? chunk : tile;
     if (P.mfit + 2 > w) w = P.mfit + 2;
+    if (kSortSeg > w) w = kSortSeg;  // sort keys (uint64) before the point loop
+    PSB_TAKE(perm, kSortSeg / 2)
     PSB_TAKE(work, w)
 #undef PSB_TAKE
     L.ipiv = o;
@@ -76,6 +79,61 @@ enum {
     M_P3 = 10,
     M_WORK = 11
 };
+
+// Order the points [s0, s0 + len) by the direction of the Sun-Earth bisector
+// in the body frame (equal-area latitude bands, longitude in alternating
+// direction), so that the 32 points of a warp see nearly the same facets and
+// a warp skips a facet whenever none of its points sees it.  Only the
+// assignment of points to threads changes: every point's sums, and so every
+// result, are the same in any order.  perm[i] receives the i-th point.
+__device__ void sort_points(const DevProblem& P, int s0, int len, const double* B, double omg,
+                            unsigned long long* keys, int* perm) {
+    int n2 = 1;
+    while (n2 < len) n2 <<= 1;
+    const int nw = (len + 31) / 32;
+    int nb = (int)(sqrt((double)nw / 1.5) + 0.5);
+    if (nb < 1) nb = 1;
+    for (int i = threadIdx.x; i < n2; i += kThreads) {
+        unsigned long long key = ~0ull;
+        if (i < len) {
+            const int p = s0 + i;
+            const double f = fmod(omg * P.t[p] + P.phi0, 2 * kPiD);
+            const double cf = cos(f), sf = sin(f);
+            const double bx = P.ex[p] + P.e0x[p], by = P.ey[p] + P.e0y[p], bz = P.ez[p] + P.e0z[p];
+            const double w0 = B[0] * bx + B[1] * by + B[2] * bz;
+            const double w1 = B[3] * bx + B[4] * by + B[5] * bz;
+            const double z = B[6] * bx + B[7] * by + B[8] * bz;
+            const double x = cf * w0 + sf * w1, y = cf * w1 - sf * w0;
+            const double r = sqrt(x * x + y * y + z * z);
+            const double c = r > 0 ? z / r : 1.0;
+            int band = (int)((1.0 - c) * 0.5 * nb);
+            band = band < 0 ? 0 : (band >= nb ? nb - 1 : band);
+            const double ax = fabs(x) + fabs(y);
+            double pa = ax > 0 ? (y >= 0 ? 1.0 - x / ax : 3.0 + x / ax) : 0.0;  // pseudo-angle in [0, 4]
+            if (band & 1) pa = 4.0 - pa;
+            const float kf = (float)(band * 8 + pa + 0.5);
+            key = ((unsigned long long)__float_as_uint(kf) << 32) | (unsigned)p;
+        }
+        keys[i] = key;
+    }
+    __syncthreads();
+    for (int k = 2; k <= n2; k <<= 1)
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = threadIdx.x; i < n2; i += kThreads) {
+                const int ixj = i ^ j;
+                if (ixj > i) {
+                    const unsigned long long a = keys[i], b = keys[ixj];
+                    if ((a > b) == ((i & k) == 0)) {
+                        keys[i] = b;
+                        keys[ixj] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int i = threadIdx.x; i < len; i += kThreads) perm[i] = (int)(keys[i] & 0xffffffffu);
+    __syncthreads();
+}
 
 // One model evaluation, the reference's mrqcof (mrqcof.c:16-148) at
 // parameters a (shared memory).  Writes the symmetrised alpha and beta into
@@ -155,13 +213,19 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
             dres[nc * C + j] = s;
         }
     }
-    // bright.c:54-125 for every data point
+    // bright.c:54-125 for every data point, in segments of points sorted by
+    // viewing direction
     double* s_fac = work;
     double* s_dg = work + kFch * 5;
+    int* perm = (int*)(sm + L.perm);
     const double cl = misc[M_CL], cls = misc[M_CLS];
-    for (int base = 0; base < P.n_points; base += kThreads) {
-        const int p = base + tid;
-        const bool act = p < P.n_points;
+    for (int s0 = 0; s0 < P.n_points; s0 += kSortSeg) {
+    const int seg = min(kSortSeg, P.n_points - s0);
+    __syncthreads();
+    sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
+    for (int base = 0; base < seg; base += kThreads) {
+        const bool act = base + tid < seg;
+        const int p = act ? perm[base + tid] : 0;
         PointGeom G;
         if (act) point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
         double acc[NCB];
@@ -282,6 +346,7 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
             Jt[(size_t)(C + 7) * npad + p] = sc * s_cls;
             yt[p] = br * sc;
         }
+    }
     }
     __syncthreads();
     // convexity rows (conv.c:12-29): y = residual, J = dres for the shape
