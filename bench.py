@@ -166,7 +166,7 @@ def _c4_worker(args):
 
 
 def run_c4(args, local):
-    """Uneven batch: many asteroids, point counts
+    """Uneven multi-asteroid batch: many asteroids, point counts
     log-uniform in 100-5000, dense/sparse mix, lmax = 6, nrows = 10,
     per-fit convergence, all in one persistent launch replayed from a CUDA
     graph.  A step scans `periods` consecutive trial periods of every

@@ -7,7 +7,7 @@
  * format (period_search_BOINC.cpp:926-931, "%.8f  %.6f  %.6f %4.1f %4.0f
  * %4.0f") passes six doubles, so the side file carries the same six values
  * unrounded: 24*per_best, dev_best, dev_best^2*(ndata-3), dark (or conw on
- * line 1), lambda, beta.  This is how parity is judged at 1e-9 instead of at
+ * line 1), lambda, beta.  This is how parity is checked at 1e-9 instead of at
  * the printed digits.
  *
  * Test infrastructure: built into oracle/_ref/, never shipped.

@@ -1,8 +1,7 @@
 """Sharding trial periods across GPUs (one process per GPU).
 
-Trial periods are independent units (README.md:12 of the
-reference: "the period interval can be divided into smaller parts"), so a
-multi-GPU scan gives each rank disjoint blocks of consecutive periods and
+Trial periods are independent units (README.md:12 of the reference: "the
+period interval can be divided into smaller parts"), so a multi-GPU scan gives each rank disjoint blocks of consecutive periods and
 needs no collective on the data path: the only exchange is the final
 ordered gather of the 48-byte records to the writer.  Blocks are dealt
 round-robin (block b goes to rank b % world), which balances uneven

@@ -289,7 +289,7 @@ def _tiny_rel(seed=8, n_periods=3):
 
 
 def c4_asteroid(i: int, periods: int | None = None):
-    """Asteroid i of the uneven batch: N log-uniform in
+    """Asteroid i of the uneven multi-asteroid batch: N log-uniform in
     100-5000, dense/sparse split U(0,1) (dense nights of 40-80 points),
     lmax = mmax = 6, nrows = 10, a period window of U(5 %, 50 %) of 2-100 h
     around the true period at the reference step rule, and the per-fit
