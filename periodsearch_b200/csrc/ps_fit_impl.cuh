@@ -52,6 +52,7 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     PSB_TAKE(misc, 32)
     PSB_TAKE(red, 2 * (kThreads / 32) + 2)
     int chunk = kFch * 5 + kFch * P.NCB;
+    if (2 * kFch * (4 + P.NCB) > chunk) chunk = 2 * kFch * (4 + P.NCB);  // fast form: two staged chunks
     int tile = kRt * (P.mfit + 1) + kRt * (P.mfit + 2);
     int w = chunk > tile ? chunk : tile;
     if (P.mfit + 2 > w) w = P.mfit + 2;
@@ -135,6 +136,210 @@ __device__ void sort_points(const DevProblem& P, int s0, int len, const double* 
     __syncthreads();
 }
 
+// One FP64 tensor-core step, D = A B + D with A 8x4 (row), B 4x8 (col):
+// lane l holds A[l/4][l%4], B[l%4][l/4] and D[l/4][2(l%4)], D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Stage facets [f0, f0 + kFch) of the facet table (nx, ny, nz, Darea) and of
+// dsph into one chunk buffer: asynchronous 16-byte copies, zeros past F.
+template <int NCB>
+__device__ __forceinline__ void stage_chunk_async(const DevProblem& P, int f0, double* fb, double* db) {
+    const int nf = min(kFch, P.F - f0);
+    const double* fs = P.fac + (size_t)f0 * 4;
+    const double* ds = P.dsph + (size_t)f0 * NCB;
+    for (int i = threadIdx.x; i < kFch * 2; i += kThreads) {
+        if (i < nf * 2)
+            cp_async16(fb + 2 * i, fs + 2 * i);
+        else
+            reinterpret_cast<double2*>(fb)[i] = make_double2(0.0, 0.0);
+    }
+    for (int i = threadIdx.x; i < kFch * (NCB / 2); i += kThreads) {
+        if (i < nf * (NCB / 2))
+            cp_async16(db + 2 * i, ds + 2 * i);
+        else
+            reinterpret_cast<double2*>(db)[i] = make_double2(0.0, 0.0);
+    }
+    cp_async_commit();
+}
+
+// bright.c:54-125 for every data point, fast form, with the shape sums on the
+// FP64 tensor cores.  The shape derivatives are a matrix product,
+//   dyda[p][k] = sum_f (Darea_f s_pf) (g_f dsph[f][k]) = sum_f A[p][f] dsph[f][k]
+// with A[p][f] = Area_f s_pf for the facets p sees (0 otherwise).  A warp owns
+// kMT tiles of 8 points; per step of 4 facets lane (g, q) forms A for point g
+// and facet q of each tile -- visibility, s, and the brightness, rotation and
+// scattering sums over its facets -- and the warp multiplies the 8x4 A tile
+// into the 8 x NCB accumulator tiles with m8n8k4 FP64 MMAs (B = dsph rows from
+// shared memory).  A tile with no visible (point, facet) pair in the step
+// skips its MMAs.  Facet chunks are staged with asynchronous copies, one chunk
+// ahead.  Sums split by facet (lane q takes facets q mod 4) are combined at
+// the end: the form differs from the reference order by rounding only.
+template <int NCB>
+__device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm, const Layout& L, const double* B,
+                                                const double* D, const double* misc, const double* area,
+                                                double* work, double* Jt, double* yt) {
+    constexpr int NT = NCB / 8;                  // accumulator tiles per 8 points
+    constexpr int kMT = 1;                       // point tiles per warp
+    constexpr int kPts = (kThreads / 32) * 8 * kMT;  // points per pass
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, q = lane & 3;
+    const int F = P.F, C = P.C, npad = P.npad;
+    double* fbuf[2] = {work, work + kFch * (4 + NCB)};
+    double* dbuf[2] = {work + kFch * 4, work + kFch * (4 + NCB) + kFch * 4};
+    int* perm = (int*)(sm + L.perm);
+    const double cl = misc[M_CL], cls = misc[M_CLS];
+    const unsigned full = 0xffffffffu;
+    const int nch = (F + kFch - 1) / kFch;
+    for (int s0 = 0; s0 < P.n_points; s0 += kSortSeg) {
+        const int seg = min(kSortSeg, P.n_points - s0);
+        __syncthreads();
+        sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
+        for (int base = 0; base < seg; base += kPts) {
+            int p[kMT];
+            bool act[kMT];
+            double e[kMT][3], e0[kMT][3];
+#pragma unroll
+            for (int i = 0; i < kMT; i++) {
+                const int ps = base + warp * 8 * kMT + i * 8 + g;
+                act[i] = ps < seg;
+                p[i] = act[i] ? perm[ps] : 0;
+#pragma unroll
+                for (int c = 0; c < 3; c++) e[i][c] = e0[i][c] = 0;
+                if (act[i]) {
+                    PointGeom G;
+                    point_geometry(P, p[i], B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        e[i][c] = G.e[c];
+                        e0[i][c] = G.e0[c];
+                    }
+                }
+            }
+            double acc[kMT][NT][2];
+            double br[kMT], T[kMT][3], S[kMT][3], s_cl[kMT], s_cls[kMT];
+#pragma unroll
+            for (int i = 0; i < kMT; i++) {
+#pragma unroll
+                for (int t = 0; t < NT; t++) acc[i][t][0] = acc[i][t][1] = 0;
+                br[i] = s_cl[i] = s_cls[i] = 0;
+#pragma unroll
+                for (int c = 0; c < 3; c++) T[i][c] = S[i][c] = 0;
+            }
+            __syncthreads();
+            stage_chunk_async<NCB>(P, 0, fbuf[0], dbuf[0]);
+            cp_async_wait_all();
+            __syncthreads();
+            for (int ch = 0; ch < nch; ch++) {
+                const int f0 = ch * kFch;
+                if (ch + 1 < nch) stage_chunk_async<NCB>(P, f0 + kFch, fbuf[(ch + 1) & 1], dbuf[(ch + 1) & 1]);
+                const double* fb = fbuf[ch & 1];
+                const double* db = dbuf[ch & 1];
+                const int nf = min(kFch, F - f0);
+                for (int j = 0; j < nf; j += 4) {
+                    const int ff = j + q;
+                    const bool valid = f0 + ff < F;
+                    const double nx = fb[ff * 4 + 0], ny = fb[ff * 4 + 1], nz = fb[ff * 4 + 2];
+                    const double ar = valid ? area[f0 + ff] : 0.0;
+                    double av[kMT];
+                    bool any[kMT];
+#pragma unroll
+                    for (int i = 0; i < kMT; i++) {
+                        const double mu = e[i][0] * nx + e[i][1] * ny + e[i][2] * nz;
+                        const double mu0 = e0[i][0] * nx + e0[i][1] * ny + e0[i][2] * nz;
+                        const bool vis = act[i] && valid && (mu > kTinyD) && (mu0 > kTinyD);
+                        any[i] = __any_sync(full, vis);
+                        av[i] = 0;
+                        if (vis) {
+                            const double r = 1.0 / (mu + mu0);
+                            const double sv = mu * mu0 * fma(cls, r, cl);
+                            av[i] = ar * sv;
+                            br[i] += av[i];
+                            const double q0 = mu0 * r, q1 = mu * r;
+                            const double w = ar * fma(cls * q0, q0, cl * mu0);
+                            const double w0 = ar * fma(cls * q1, q1, cl * mu);
+                            T[i][0] = fma(w, nx, T[i][0]);
+                            T[i][1] = fma(w, ny, T[i][1]);
+                            T[i][2] = fma(w, nz, T[i][2]);
+                            S[i][0] = fma(w0, nx, S[i][0]);
+                            S[i][1] = fma(w0, ny, S[i][1]);
+                            S[i][2] = fma(w0, nz, S[i][2]);
+                            const double mm = mu * mu0 * ar;
+                            s_cl[i] += mm;
+                            s_cls[i] = fma(mm, r, s_cls[i]);
+                        }
+                    }
+                    bool some = false;
+#pragma unroll
+                    for (int i = 0; i < kMT; i++) some = some || any[i];
+                    if (!some) continue;
+                    const double* brow = db + ff * NCB + g;
+#pragma unroll
+                    for (int t = 0; t < NT; t++) {
+                        const double bv = brow[t * 8];
+#pragma unroll
+                        for (int i = 0; i < kMT; i++)
+                            if (any[i]) dmma_8x8x4(acc[i][t][0], acc[i][t][1], av[i], bv);
+                    }
+                }
+                cp_async_wait_all();
+                __syncthreads();
+            }
+#pragma unroll
+            for (int i = 0; i < kMT; i++) {
+                // the four lanes of a point hold the sums over facets q mod 4
+#pragma unroll
+                for (int o = 1; o <= 2; o <<= 1) {
+                    br[i] += __shfl_xor_sync(full, br[i], o);
+                    s_cl[i] += __shfl_xor_sync(full, s_cl[i], o);
+                    s_cls[i] += __shfl_xor_sync(full, s_cls[i], o);
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        T[i][c] += __shfl_xor_sync(full, T[i][c], o);
+                        S[i][c] += __shfl_xor_sync(full, S[i][c], o);
+                    }
+                }
+                if (!act[i]) continue;
+                PointGeom G;
+                point_geometry(P, p[i], B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
+                const double sc = G.scale;
+#pragma unroll
+                for (int t = 0; t < NT; t++)
+#pragma unroll
+                    for (int jj = 0; jj < 2; jj++) {
+                        const int k = t * 8 + 2 * q + jj;
+                        if (k < C) Jt[(size_t)k * npad + p[i]] = sc * acc[i][t][jj];
+                    }
+                if (q == 0) {
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        double v = 0;
+#pragma unroll
+                        for (int c = 0; c < 3; c++) v = fma(T[i][c], G.de[c][k], fma(S[i][c], G.de0[c][k], v));
+                        Jt[(size_t)(C + k) * npad + p[i]] = sc * v;
+                    }
+                    Jt[(size_t)(C + 3) * npad + p[i]] = br[i] * G.dphp[0];
+                    Jt[(size_t)(C + 4) * npad + p[i]] = br[i] * G.dphp[1];
+                    Jt[(size_t)(C + 5) * npad + p[i]] = br[i] * G.dphp[2];
+                    Jt[(size_t)(C + 6) * npad + p[i]] = sc * s_cl[i] * cl;
+                    Jt[(size_t)(C + 7) * npad + p[i]] = sc * s_cls[i];
+                    yt[p[i]] = br[i] * sc;
+                }
+            }
+        }
+    }
+}
+
 // One model evaluation, the reference's mrqcof (mrqcof.c:16-148) at
 // parameters a (shared memory).  Writes the symmetrised alpha and beta into
 // alpha_out / beta_out (shared memory) and chi2, the convexity residuals
@@ -213,140 +418,144 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
             dres[nc * C + j] = s;
         }
     }
-    // bright.c:54-125 for every data point, in segments of points sorted by
-    // viewing direction
-    double* s_fac = work;
-    double* s_dg = work + kFch * 5;
-    int* perm = (int*)(sm + L.perm);
-    const double cl = misc[M_CL], cls = misc[M_CLS];
-    for (int s0 = 0; s0 < P.n_points; s0 += kSortSeg) {
-    const int seg = min(kSortSeg, P.n_points - s0);
-    __syncthreads();
-    sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
-    for (int base = 0; base < seg; base += kThreads) {
-        const bool act = base + tid < seg;
-        const int p = act ? perm[base + tid] : 0;
-        PointGeom G;
-        if (act) point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
-        double acc[NCB];
-#pragma unroll
-        for (int k = 0; k < NCB; k++) acc[k] = 0;
-        double br = 0, rot0 = 0, rot1 = 0, rot2 = 0, s_cl = 0, s_cls = 0;
-        double sS0 = 0, sS1 = 0, sS2 = 0;  // kFast: sum Area dsmu0 n
-        for (int f0 = 0; f0 < F; f0 += kFch) {
-            const int nf = min(kFch, F - f0);
-            __syncthreads();
-            for (int idx = tid; idx < nf * NCB; idx += kThreads) {
-                const int ff = idx / NCB, k = idx - ff * NCB;
-                s_dg[idx] = g[f0 + ff] * P.dsph[(size_t)(f0 + ff) * NCB + k];
-            }
-            for (int ff = tid; ff < nf; ff += kThreads) {
-                const double* fa = P.fac + (size_t)(f0 + ff) * 4;
-                s_fac[ff * 5 + 0] = fa[0];
-                s_fac[ff * 5 + 1] = fa[1];
-                s_fac[ff * 5 + 2] = fa[2];
-                s_fac[ff * 5 + 3] = area[f0 + ff];
-                s_fac[ff * 5 + 4] = fa[3];
-            }
-            __syncthreads();
-            if (act) {
-                for (int ff = 0; ff < nf; ff++) {
-                    const double nx = s_fac[ff * 5 + 0], ny = s_fac[ff * 5 + 1], nz = s_fac[ff * 5 + 2];
-                    const double mu = G.e[0] * nx + G.e[1] * ny + G.e[2] * nz;
-                    const double mu0 = G.e0[0] * nx + G.e0[1] * ny + G.e0[2] * nz;
-                    if ((mu > kTinyD) && (mu0 > kTinyD)) {
-                        const double ar = s_fac[ff * 5 + 3], darea = s_fac[ff * 5 + 4];
-                        if constexpr (kFast) {
-                            // one reciprocal; rotation derivatives through the
-                            // facet sums T = sum Area dsmu n, S = sum Area dsmu0 n
-                            const double r = 1.0 / (mu + mu0);
-                            const double s = mu * mu0 * fma(cls, r, cl);
-                            br = fma(ar, s, br);
-                            const double q0 = mu0 * r, q1 = mu * r;
-                            const double w = ar * fma(cls * q0, q0, cl * mu0);
-                            const double w0 = ar * fma(cls * q1, q1, cl * mu);
-                            rot0 = fma(w, nx, rot0);
-                            rot1 = fma(w, ny, rot1);
-                            rot2 = fma(w, nz, rot2);
-                            sS0 = fma(w0, nx, sS0);
-                            sS1 = fma(w0, ny, sS1);
-                            sS2 = fma(w0, nz, sS2);
-                            const double mm = mu * mu0 * ar;
-                            s_cl += mm;
-                            s_cls = fma(mm, r, s_cls);
-                            const double dbr = darea * s;
-                            const double* dg = s_dg + ff * NCB;
-#pragma unroll
-                            for (int k = 0; k < NCB; k++) acc[k] = fma(dbr, dg[k], acc[k]);
-                        } else {
-                            const double dnom = mu + mu0;
-                            const double s = mu * mu0 * (cl + cls / dnom);
-                            br = br + ar * s;
-                            const double q0 = mu0 / dnom, q1 = mu / dnom;
-                            const double dsmu = cls * (q0 * q0) + cl * mu0;
-                            const double dsmu0 = cls * (q1 * q1) + cl * mu;
-                            const double dbr = darea * s;
-                            const double* dg = s_dg + ff * NCB;
-#pragma unroll
-                            for (int k = 0; k < NCB; k++) acc[k] = acc[k] + dbr * dg[k];
-                            {
-                                const double sum = nx * G.de[0][0] + ny * G.de[1][0] + nz * G.de[2][0];
-                                const double sum0 = nx * G.de0[0][0] + ny * G.de0[1][0] + nz * G.de0[2][0];
-                                rot0 = rot0 + ar * (dsmu * sum + dsmu0 * sum0);
+    if constexpr (kFast) {
+        point_loop_fast<NCB>(P, sm, L, B, D, misc, area, work, Jt, yt);
+    } else {
+        // bright.c:54-125 for every data point, in segments of points sorted by
+        // viewing direction
+        double* s_fac = work;
+        double* s_dg = work + kFch * 5;
+        int* perm = (int*)(sm + L.perm);
+        const double cl = misc[M_CL], cls = misc[M_CLS];
+        for (int s0 = 0; s0 < P.n_points; s0 += kSortSeg) {
+        const int seg = min(kSortSeg, P.n_points - s0);
+        __syncthreads();
+        sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
+        for (int base = 0; base < seg; base += kThreads) {
+            const bool act = base + tid < seg;
+            const int p = act ? perm[base + tid] : 0;
+            PointGeom G;
+            if (act) point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
+            double acc[NCB];
+    #pragma unroll
+            for (int k = 0; k < NCB; k++) acc[k] = 0;
+            double br = 0, rot0 = 0, rot1 = 0, rot2 = 0, s_cl = 0, s_cls = 0;
+            double sS0 = 0, sS1 = 0, sS2 = 0;  // kFast: sum Area dsmu0 n
+            for (int f0 = 0; f0 < F; f0 += kFch) {
+                const int nf = min(kFch, F - f0);
+                __syncthreads();
+                for (int idx = tid; idx < nf * NCB; idx += kThreads) {
+                    const int ff = idx / NCB, k = idx - ff * NCB;
+                    s_dg[idx] = g[f0 + ff] * P.dsph[(size_t)(f0 + ff) * NCB + k];
+                }
+                for (int ff = tid; ff < nf; ff += kThreads) {
+                    const double* fa = P.fac + (size_t)(f0 + ff) * 4;
+                    s_fac[ff * 5 + 0] = fa[0];
+                    s_fac[ff * 5 + 1] = fa[1];
+                    s_fac[ff * 5 + 2] = fa[2];
+                    s_fac[ff * 5 + 3] = area[f0 + ff];
+                    s_fac[ff * 5 + 4] = fa[3];
+                }
+                __syncthreads();
+                if (act) {
+                    for (int ff = 0; ff < nf; ff++) {
+                        const double nx = s_fac[ff * 5 + 0], ny = s_fac[ff * 5 + 1], nz = s_fac[ff * 5 + 2];
+                        const double mu = G.e[0] * nx + G.e[1] * ny + G.e[2] * nz;
+                        const double mu0 = G.e0[0] * nx + G.e0[1] * ny + G.e0[2] * nz;
+                        if ((mu > kTinyD) && (mu0 > kTinyD)) {
+                            const double ar = s_fac[ff * 5 + 3], darea = s_fac[ff * 5 + 4];
+                            if constexpr (kFast) {
+                                // one reciprocal; rotation derivatives through the
+                                // facet sums T = sum Area dsmu n, S = sum Area dsmu0 n
+                                const double r = 1.0 / (mu + mu0);
+                                const double s = mu * mu0 * fma(cls, r, cl);
+                                br = fma(ar, s, br);
+                                const double q0 = mu0 * r, q1 = mu * r;
+                                const double w = ar * fma(cls * q0, q0, cl * mu0);
+                                const double w0 = ar * fma(cls * q1, q1, cl * mu);
+                                rot0 = fma(w, nx, rot0);
+                                rot1 = fma(w, ny, rot1);
+                                rot2 = fma(w, nz, rot2);
+                                sS0 = fma(w0, nx, sS0);
+                                sS1 = fma(w0, ny, sS1);
+                                sS2 = fma(w0, nz, sS2);
+                                const double mm = mu * mu0 * ar;
+                                s_cl += mm;
+                                s_cls = fma(mm, r, s_cls);
+                                const double dbr = darea * s;
+                                const double* dg = s_dg + ff * NCB;
+    #pragma unroll
+                                for (int k = 0; k < NCB; k++) acc[k] = fma(dbr, dg[k], acc[k]);
+                            } else {
+                                const double dnom = mu + mu0;
+                                const double s = mu * mu0 * (cl + cls / dnom);
+                                br = br + ar * s;
+                                const double q0 = mu0 / dnom, q1 = mu / dnom;
+                                const double dsmu = cls * (q0 * q0) + cl * mu0;
+                                const double dsmu0 = cls * (q1 * q1) + cl * mu;
+                                const double dbr = darea * s;
+                                const double* dg = s_dg + ff * NCB;
+    #pragma unroll
+                                for (int k = 0; k < NCB; k++) acc[k] = acc[k] + dbr * dg[k];
+                                {
+                                    const double sum = nx * G.de[0][0] + ny * G.de[1][0] + nz * G.de[2][0];
+                                    const double sum0 = nx * G.de0[0][0] + ny * G.de0[1][0] + nz * G.de0[2][0];
+                                    rot0 = rot0 + ar * (dsmu * sum + dsmu0 * sum0);
+                                }
+                                {
+                                    const double sum = nx * G.de[0][1] + ny * G.de[1][1] + nz * G.de[2][1];
+                                    const double sum0 = nx * G.de0[0][1] + ny * G.de0[1][1] + nz * G.de0[2][1];
+                                    rot1 = rot1 + ar * (dsmu * sum + dsmu0 * sum0);
+                                }
+                                {
+                                    const double sum = nx * G.de[0][2] + ny * G.de[1][2] + nz * G.de[2][2];
+                                    const double sum0 = nx * G.de0[0][2] + ny * G.de0[1][2] + nz * G.de0[2][2];
+                                    rot2 = rot2 + ar * (dsmu * sum + dsmu0 * sum0);
+                                }
+                                s_cl = s_cl + mu * mu0 * ar;
+                                s_cls = s_cls + ar * mu * mu0 / (mu + mu0);
                             }
-                            {
-                                const double sum = nx * G.de[0][1] + ny * G.de[1][1] + nz * G.de[2][1];
-                                const double sum0 = nx * G.de0[0][1] + ny * G.de0[1][1] + nz * G.de0[2][1];
-                                rot1 = rot1 + ar * (dsmu * sum + dsmu0 * sum0);
-                            }
-                            {
-                                const double sum = nx * G.de[0][2] + ny * G.de[1][2] + nz * G.de[2][2];
-                                const double sum0 = nx * G.de0[0][2] + ny * G.de0[1][2] + nz * G.de0[2][2];
-                                rot2 = rot2 + ar * (dsmu * sum + dsmu0 * sum0);
-                            }
-                            s_cl = s_cl + mu * mu0 * ar;
-                            s_cls = s_cls + ar * mu * mu0 / (mu + mu0);
                         }
                     }
                 }
             }
-        }
-        if constexpr (kFast) {
-            // rotation derivatives from the facet-summed vectors; the point
-            // geometry is recomputed so that de/de0 need no registers in the loop
-            if (act) {
-                PointGeom G2;
-                point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G2);
-                const double T[3] = {rot0, rot1, rot2}, S[3] = {sS0, sS1, sS2};
-                double rk[3];
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    double v = 0;
-#pragma unroll
-                    for (int j = 0; j < 3; j++) v = fma(T[j], G2.de[j][k], fma(S[j], G2.de0[j][k], v));
-                    rk[k] = v;
+            if constexpr (kFast) {
+                // rotation derivatives from the facet-summed vectors; the point
+                // geometry is recomputed so that de/de0 need no registers in the loop
+                if (act) {
+                    PointGeom G2;
+                    point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G2);
+                    const double T[3] = {rot0, rot1, rot2}, S[3] = {sS0, sS1, sS2};
+                    double rk[3];
+    #pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        double v = 0;
+    #pragma unroll
+                        for (int j = 0; j < 3; j++) v = fma(T[j], G2.de[j][k], fma(S[j], G2.de0[j][k], v));
+                        rk[k] = v;
+                    }
+                    rot0 = rk[0];
+                    rot1 = rk[1];
+                    rot2 = rk[2];
                 }
-                rot0 = rk[0];
-                rot1 = rk[1];
-                rot2 = rk[2];
+            }
+            if (act) {
+                const double sc = G.scale;
+    #pragma unroll
+                for (int k = 0; k < NCB; k++)
+                    if (k < C) Jt[(size_t)k * npad + p] = sc * acc[k];
+                Jt[(size_t)(C + 0) * npad + p] = sc * rot0;
+                Jt[(size_t)(C + 1) * npad + p] = sc * rot1;
+                Jt[(size_t)(C + 2) * npad + p] = sc * rot2;
+                Jt[(size_t)(C + 3) * npad + p] = br * G.dphp[0];
+                Jt[(size_t)(C + 4) * npad + p] = br * G.dphp[1];
+                Jt[(size_t)(C + 5) * npad + p] = br * G.dphp[2];
+                Jt[(size_t)(C + 6) * npad + p] = sc * s_cl * cl;
+                Jt[(size_t)(C + 7) * npad + p] = sc * s_cls;
+                yt[p] = br * sc;
             }
         }
-        if (act) {
-            const double sc = G.scale;
-#pragma unroll
-            for (int k = 0; k < NCB; k++)
-                if (k < C) Jt[(size_t)k * npad + p] = sc * acc[k];
-            Jt[(size_t)(C + 0) * npad + p] = sc * rot0;
-            Jt[(size_t)(C + 1) * npad + p] = sc * rot1;
-            Jt[(size_t)(C + 2) * npad + p] = sc * rot2;
-            Jt[(size_t)(C + 3) * npad + p] = br * G.dphp[0];
-            Jt[(size_t)(C + 4) * npad + p] = br * G.dphp[1];
-            Jt[(size_t)(C + 5) * npad + p] = br * G.dphp[2];
-            Jt[(size_t)(C + 6) * npad + p] = sc * s_cl * cl;
-            Jt[(size_t)(C + 7) * npad + p] = sc * s_cls;
-            yt[p] = br * sc;
         }
-    }
     }
     __syncthreads();
     // convexity rows (conv.c:12-29): y = residual, J = dres for the shape
@@ -444,7 +653,7 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
 }
 
 template <int NCB, bool kFast>
-__global__ void __launch_bounds__(kThreads, 1) fit_kernel(const DevProblem* __restrict__ Parr, FitBatch Bt) {
+__global__ void __launch_bounds__(kThreads, kFast ? 2 : 1) fit_kernel(const DevProblem* __restrict__ Parr, FitBatch Bt) {
     extern __shared__ __align__(16) double sm[];
     __shared__ int s_work, s_ast;
     const int tid = threadIdx.x;

@@ -108,15 +108,18 @@ def _read_full(path):
 
 
 def perturbation_spread(name, ref):
-    """Largest relative chi2 change per period among last-ulp perturbations of
-    the reference: its FMA rebuild and the restatement's perturbed builds
-    (tests/golden/make_golden.py)."""
-    spread = np.zeros(len(ref))
+    """Largest change per period among last-ulp perturbations of the
+    reference (its FMA rebuild and the restatement's perturbed builds,
+    tests/golden/make_golden.py): relative for chi2, in degrees for the pole
+    angles, which a flat chi2 valley lets move further than chi2 does."""
+    spread = np.zeros(len(ref), dtype=[("chi2", "f8"), ("lambda_deg", "f8"), ("beta_deg", "f8")])
     for f in ("fma_out.full", "var_sq.full", "var_fma.full", "var_fmasq.full"):
         path = os.path.join(GOLDEN, name, f)
         if os.path.exists(path):
             x = _read_full(path)
-            spread = np.maximum(spread, np.abs(x["chi2"] - ref["chi2"]) / np.abs(ref["chi2"]))
+            spread["chi2"] = np.maximum(spread["chi2"], np.abs(x["chi2"] - ref["chi2"]) / np.abs(ref["chi2"]))
+            for key in ("lambda_deg", "beta_deg"):
+                spread[key] = np.maximum(spread[key], np.abs(x[key] - ref[key]))
     return spread
 
 
@@ -124,11 +127,12 @@ def check_records(gpu, ref, spread, label):
     """Per-period parity with the chaotic-period triage, plus the ranking."""
     assert gpu.shape == ref.shape
     n = len(ref)
-    chaotic = spread > FIT_TOL
+    cs = spread["chi2"]
+    chaotic = cs > FIT_TOL
     err = np.abs(gpu["chi2"] - ref["chi2"]) / np.abs(ref["chi2"])
-    ok = (err <= FIT_TOL) | (chaotic & (err <= np.maximum(spread, FIT_TOL) * 10))
+    ok = (err <= FIT_TOL) | (chaotic & (err <= np.maximum(cs, FIT_TOL) * 10))
     bad = np.nonzero(~ok)[0]
-    assert len(bad) == 0, (label, [(int(i) + 1, float(err[i]), float(spread[i])) for i in bad[:10]])
+    assert len(bad) == 0, (label, [(int(i) + 1, float(err[i]), float(cs[i])) for i in bad[:10]])
     calm = ~chaotic & (err <= FIT_TOL)
     # within calm periods every field matches (record 0 col 4 is conw there)
     assert np.all(np.abs(gpu["rms"][calm] - ref["rms"][calm]) <= FIT_TOL * np.abs(ref["rms"][calm]))
@@ -137,7 +141,11 @@ def check_records(gpu, ref, spread, label):
     d[0] = 0.0
     assert np.all(d[calm] <= 1e-6), (label, float(np.max(d[calm])))
     for key in ("lambda_deg", "beta_deg"):
-        assert np.all(np.abs(gpu[key][calm] - ref[key][calm]) <= 1e-6), key
+        # 1e-6 degrees, or ten times what the reference's own perturbations move
+        tol = np.maximum(1e-6, 10 * spread[key])
+        d = np.abs(gpu[key] - ref[key])
+        assert np.all(d[calm] <= tol[calm]), (key, [(int(i) + 1, float(d[i]), float(spread[key][i]))
+                                                    for i in np.nonzero(calm & (d > tol))[0][:5]])
     for k in (1, min(10, n), min(20, n)):
         assert list(np.argsort(gpu["chi2"], kind="stable")[:k]) == list(np.argsort(ref["chi2"], kind="stable")[:k])
     return int(chaotic.sum()), float(err.max())
