@@ -31,7 +31,7 @@ int fast_max_blocks_per_sm(const DevProblem& P, int* threads) {
 }
 
 cudaError_t launch_fast_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s) {
-    if (P.nq <= 0 || P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 > fitimpl::kMaxEpt * fitcommon::kThreads) return cudaErrorInvalidValue;
+    if (P.nq <= 0 || fitimpl::alpha_job_count(P.mfit) > fitimpl::kJobs * fitcommon::kThreads) return cudaErrorInvalidValue;
     switch (P.NCB) {
         case 8: return fitimpl::launch_fits_t<8, true>(P, dP, B, grid, s);
         case 16: return fitimpl::launch_fits_t<16, true>(P, dP, B, grid, s);
@@ -46,7 +46,7 @@ cudaError_t launch_fast_fits(const DevProblem& P, const DevProblem* dP, const Fi
 }
 
 cudaError_t launch_fast_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s) {
-    if (P.nq <= 0 || P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 > fitimpl::kMaxEpt * fitcommon::kThreads) return cudaErrorInvalidValue;
+    if (P.nq <= 0 || fitimpl::alpha_job_count(P.mfit) > fitimpl::kJobs * fitcommon::kThreads) return cudaErrorInvalidValue;
     switch (P.NCB) {
         case 8: return fitimpl::launch_eval_t<8, true>(P, dP, E, s);
         case 16: return fitimpl::launch_eval_t<16, true>(P, dP, E, s);

@@ -112,104 +112,188 @@ __device__ __forceinline__ void point_geometry(const DevProblem& P, int p, const
     }
 }
 
-// Block-wide argmax of |a| candidates with the reference's tie rule: the
-// largest value wins, among equal values the largest linear index (the last
-// one met in row-major scan order, gauss_errc.c:21-28).  idx < 0 = none.
-__device__ void block_argmax(double& v, int& idx, double* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        double ov = __shfl_down_sync(0xffffffffu, v, o);
-        int oi = __shfl_down_sync(0xffffffffu, idx, o);
-        if (oi >= 0 && (idx < 0 || ov > v || (ov == v && oi > idx))) {
-            v = ov;
-            idx = oi;
-        }
-    }
-    int* redi = (int*)(red + kThreads / 32);
-    if (lane == 0) {
-        red[warp] = v;
-        redi[warp] = idx;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double bv = red[0];
-        int bi = redi[0];
-        for (int w = 1; w < kThreads / 32; w++) {
-            if (redi[w] >= 0 && (bi < 0 || red[w] > bv || (red[w] == bv && redi[w] > bi))) {
-                bv = red[w];
-                bi = redi[w];
-            }
-        }
-        red[kThreads / 16] = bv;
-        ((int*)(red + kThreads / 16 + 1))[0] = bi;
-    }
-    __syncthreads();
-    v = red[kThreads / 16];
-    idx = ((int*)(red + kThreads / 16 + 1))[0];
-}
+// Words of shared memory gauss_jordan needs in buf for an n x n system.
+__host__ __device__ constexpr int gj_buf_doubles(int n) { return 3 * n + 4 + 4 * (kThreads / 32); }
 
-// gauss_errc.c:9-73 on the n x n row-major matrix a (shared memory) with
-// right-hand side b; the solution replaces b.  Returns 0, 1 or 2, the same
-// value in every thread.  The final column unscrambling of the inverse is
-// omitted: mrqmin (mrqmin.c:59-76) only uses b.
-__device__ int gauss_jordan(double* a, double* b, int n, int* ipiv, double* dum, double* red) {
-    const int tid = threadIdx.x;
-    for (int j = tid; j < n; j += kThreads) ipiv[j] = 0;
-    __syncthreads();
-    for (int i = 0; i < n; i++) {
+// Register tile of gauss_jordan for systems of at most nmax unknowns: rows
+// warp + 8 r (r < kR), columns lane + 32 c (c < kC), column n standing for b.
+template <int nmax>
+struct GjTile {
+    static constexpr int kW = kThreads / 32;
+    static constexpr int kR = (nmax + kW - 1) / kW;
+    static constexpr int kC = (nmax + 1 + 31) / 32;
+};
+
+// gauss_errc.c:9-73 on the n x n row-major matrix a (shared memory,
+// n <= nmax <= 72) with right-hand side b; the solution replaces b, a is left
+// undefined.  Returns 0, 1 or 2, the same value in every thread.  The final
+// column unscrambling of the inverse is omitted: mrqmin (mrqmin.c:59-76) only
+// uses b.
+//
+// Full pivoting as in the reference: the pivot is the last element of largest
+// magnitude, in row-major order, among rows and columns not yet pivoted; a
+// NaN never wins.  Magnitudes are compared as unsigned integers (the bit
+// patterns of non-negative doubles are ordered like their values).  Thread
+// (warp, lane) holds the elements (warp + 8 r, lane + 32 c) in registers and
+// looks for the next pivot while it updates them; per pivot the owners
+// publish the pivot row, the row it is swapped with and the pivot column to
+// buf, so a step costs two block barriers.  Every element receives the
+// reference's operations in the reference's order: the swap,
+// a[icol][l] * pivinv, then a[ll][l] - a[icol][l] * dum.
+template <int nmax>
+__device__ int gauss_jordan(double* a, double* b, int n, double* buf) {
+    using T = GjTile<nmax>;
+    constexpr int kW = T::kW, kR = T::kR, kC = T::kC;
+    static_assert(nmax <= 72 && kR <= 32, "tile");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* prow = buf;              // pivot row before the step, [n] = b
+    double* orow = buf + n + 1;      // row icol before the step, [n] = b
+    double* colv = buf + 2 * n + 2;  // column icol before the step
+    unsigned long long* pk = (unsigned long long*)(buf + 3 * n + 4);  // per-warp keys, two generations
+    int* pidx = (int*)(pk + 2 * kW);
+    double x[kR][kC];
+    unsigned rlive = 0, clive = 0;  // owned rows / matrix columns not yet pivoted
+#pragma unroll
+    for (int r = 0; r < kR; r++) {
+        const int j = warp + kW * r;
+        if (j < n) rlive |= 1u << r;
+#pragma unroll
+        for (int c = 0; c < kC; c++) {
+            const int l = lane + 32 * c;
+            x[r][c] = (j < n && l <= n) ? (l < n ? a[j * n + l] : b[j]) : 0.0;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < kC; c++)
+        if (lane + 32 * c < n) clive |= 1u << c;
+    // candidate over the rows not yet pivoted: the last maximum of |x| in the
+    // owned row-major order (>= as in the reference; a NaN never compares),
+    // returned as key = |x| bits + 1 (0: none) and its element index
+    auto candidate = [&](unsigned long long& bk, int& bi) {
         double bv = -1.0;
-        int bi = -1;
-        for (int idx = tid; idx < n * n; idx += kThreads) {
-            const int j = idx / n, k = idx - j * n;
-            if (ipiv[j] != 1 && ipiv[k] == 0) {
-                const double v = fabs(a[idx]);
-                if (v >= bv) {
-                    bv = v;
-                    bi = idx;
-                }
+        int bs = -1;
+        bool cl[kC];
+#pragma unroll
+        for (int c = 0; c < kC; c++) cl[c] = (clive >> c) & 1u;
+#pragma unroll
+        for (int r = 0; r < kR; r++) {
+            if (!((rlive >> r) & 1u)) continue;
+#pragma unroll
+            for (int c = 0; c < kC; c++) {
+                const double v = fabs(x[r][c]);
+                const bool take = cl[c] && v >= bv;
+                bv = take ? v : bv;
+                bs = take ? r * kC + c : bs;
             }
         }
-        block_argmax(bv, bi, red);
-        if (bi < 0) return 1;  // only NaNs left: the reference ends in error 1
+        bk = bs >= 0 ? (unsigned long long)__double_as_longlong(bv) + 1 : 0ull;
+        bi = bs >= 0 ? (warp + kW * (bs / kC)) * n + lane + 32 * (bs % kC) : -1;
+    };
+    auto warp_max = [&](unsigned long long& bk, int& bi) {
+        const unsigned hi = __reduce_max_sync(0xffffffffu, (unsigned)(bk >> 32));
+        const unsigned lo = __reduce_max_sync(0xffffffffu, (unsigned)(bk >> 32) == hi ? (unsigned)bk : 0u);
+        const bool top = (unsigned)(bk >> 32) == hi && (unsigned)bk == lo;
+        bi = (int)__reduce_max_sync(0xffffffffu, top ? (unsigned)(bi + 1) : 0u) - 1;
+        bk = ((unsigned long long)hi << 32) | lo;
+    };
+    unsigned long long bk;
+    int bi;
+    candidate(bk, bi);
+    for (int i = 0; i < n; i++) {
+        warp_max(bk, bi);
+        const int gen = (i & 1) * kW;
+        if (lane == 0) {
+            pk[gen + warp] = bk;
+            pidx[gen + warp] = bi;
+        }
+        __syncthreads();
+        bk = lane < kW ? pk[gen + lane] : 0ull;
+        bi = lane < kW ? pidx[gen + lane] : -1;
+        warp_max(bk, bi);
+        if (bk == 0) return 1;  // only NaNs left: the reference ends in error 1
         const int irow = bi / n, icol = bi - irow * n;
-        __syncthreads();
-        if (tid == 0) ++ipiv[icol];
-        if (irow != icol) {
-            for (int l = tid; l < n; l += kThreads) {
-                const double tmp = a[irow * n + l];
-                a[irow * n + l] = a[icol * n + l];
-                a[icol * n + l] = tmp;
-            }
-            if (tid == 0) {
-                const double tmp = b[irow];
-                b[irow] = b[icol];
-                b[icol] = tmp;
-            }
+        // owners publish rows irow, icol and column icol
+        if ((irow & (kW - 1)) == warp) {
+            const int rr = irow / kW;
+#pragma unroll
+            for (int r = 0; r < kR; r++)
+                if (r == rr) {
+#pragma unroll
+                    for (int c = 0; c < kC; c++)
+                        if (lane + 32 * c <= n) prow[lane + 32 * c] = x[r][c];
+                }
+        }
+        if ((icol & (kW - 1)) == warp) {
+            const int rr = icol / kW;
+#pragma unroll
+            for (int r = 0; r < kR; r++)
+                if (r == rr) {
+#pragma unroll
+                    for (int c = 0; c < kC; c++)
+                        if (lane + 32 * c <= n) orow[lane + 32 * c] = x[r][c];
+                }
+        }
+        if ((icol & 31) == lane) {
+            const int cc = icol >> 5;
+#pragma unroll
+            for (int c = 0; c < kC; c++)
+                if (c == cc) {
+#pragma unroll
+                    for (int r = 0; r < kR; r++)
+                        if (warp + kW * r < n) colv[warp + kW * r] = x[r][c];
+                }
         }
         __syncthreads();
-        const double piv = a[icol * n + icol];
+        const double piv = prow[icol];
         if (piv == 0.0) return 2;
         const double pivinv = 1.0 / piv;
-        __syncthreads();
-        if (tid == 0) a[icol * n + icol] = 1.0;
-        __syncthreads();
-        for (int l = tid; l < n; l += kThreads) a[icol * n + l] *= pivinv;
-        if (tid == 0) b[icol] *= pivinv;
-        __syncthreads();
-        for (int ll = tid; ll < n; ll += kThreads) dum[ll] = a[ll * n + icol];
-        __syncthreads();
-        for (int ll = tid; ll < n; ll += kThreads)
-            if (ll != icol) a[ll * n + icol] = 0.0;
-        __syncthreads();
-        for (int idx = tid; idx < n * n; idx += kThreads) {
-            const int ll = idx / n, l = idx - ll * n;
-            if (ll != icol) a[idx] -= a[icol * n + l] * dum[ll];
+        double pr[kC], orv[kC];
+#pragma unroll
+        for (int c = 0; c < kC; c++) {
+            const int l = lane + 32 * c;
+            pr[c] = l <= n ? (l == icol ? 1.0 : prow[l]) * pivinv : 0.0;
+            orv[c] = l <= n ? (l == icol ? 0.0 : orow[l]) : 0.0;
         }
-        for (int ll = tid; ll < n; ll += kThreads)
-            if (ll != icol) b[ll] -= b[icol] * dum[ll];
-        __syncthreads();
+        const double odum = orow[icol];
+        // the pivot leaves the live set before the next search
+        if ((icol & (kW - 1)) == warp) rlive &= ~(1u << (icol / kW));
+        if ((icol & 31) == lane) {
+            const int cc = icol >> 5;
+            clive &= ~(1u << cc);
+            // a[ll][icol] = 0 before the reduction (its old value is in colv)
+#pragma unroll
+            for (int c = 0; c < kC; c++)
+                if (c == cc) {
+#pragma unroll
+                    for (int r = 0; r < kR; r++) x[r][c] = 0.0;
+                }
+        }
+#pragma unroll
+        for (int r = 0; r < kR; r++) {
+            const int j = warp + kW * r;
+            if (j >= n) continue;
+            if (j == icol) {
+#pragma unroll
+                for (int c = 0; c < kC; c++) x[r][c] = pr[c];
+            } else if (j == irow) {
+#pragma unroll
+                for (int c = 0; c < kC; c++) x[r][c] = orv[c] - pr[c] * odum;
+            } else {
+                const double dum = colv[j];
+#pragma unroll
+                for (int c = 0; c < kC; c++) x[r][c] = x[r][c] - pr[c] * dum;
+            }
+        }
+        candidate(bk, bi);
     }
+#pragma unroll
+    for (int r = 0; r < kR; r++)
+#pragma unroll
+        for (int c = 0; c < kC; c++) {
+            const int j = warp + kW * r, l = lane + 32 * c;
+            if (j < n && l == n) b[j] = x[r][c];
+        }
+    __syncthreads();
     return 0;
 }
 

@@ -23,7 +23,7 @@ using namespace fitcommon;
 
 constexpr int kFch = 32;     // facets per shared-memory chunk
 constexpr int kRt = 32;      // rows per alpha tile
-constexpr int kMaxEpt = 16;  // alpha/beta/chi2 entries per thread
+constexpr int kJobs = 2;     // alpha/beta/chi2 blocks per thread
 constexpr int kSortSeg = 1024;  // points sorted together by viewing direction
 
 // Shared-memory layout, offsets in doubles.
@@ -53,10 +53,12 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     PSB_TAKE(red, 2 * (kThreads / 32) + 2)
     int chunk = kFch * 5 + kFch * P.NCB;
     if (2 * kFch * (4 + P.NCB) > chunk) chunk = 2 * kFch * (4 + P.NCB);  // fast form: two staged chunks
-    int tile = kRt * (P.mfit + 1) + kRt * (P.mfit + 2);
+    const int kB = (P.mfit + 1) & ~1;
+    int tile = kRt * (kB + 2) + kRt * (kB + 4);  // alpha tiles Ws, Js
     int w = chunk > tile ? chunk : tile;
     if (P.mfit + 2 > w) w = P.mfit + 2;
     if (kSortSeg > w) w = kSortSeg;  // sort keys (uint64) before the point loop
+    if (gj_buf_doubles(P.mfit) > w) w = gj_buf_doubles(P.mfit);  // Gauss-Jordan buffers
     PSB_TAKE(perm, kSortSeg / 2)
     PSB_TAKE(work, w)
 #undef PSB_TAKE
@@ -65,6 +67,33 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     const int nent = P.mfit * (P.mfit + 1) / 2 + P.mfit + 1;
     L.bytes = (size_t)L.ent * sizeof(double) + (size_t)nent * sizeof(int);
     return L;
+}
+
+// Blocks of the alpha/beta/chi2 accumulation for mfit free parameters: for
+// each even j0 <= mfit - 1, the 4-column blocks k0 = 4 kb of the lower
+// triangle (k0 <= j0 + 1) and the beta block k0 = kB; then the chi2 block
+// (jC, kB), kB = jC = mfit rounded up to even.  Packed as j0 | k0 << 16.
+__host__ __device__ inline int alpha_job_count(int mfit) {
+    int n = 1;
+    for (int j0 = 0; j0 < mfit; j0 += 2) {
+        const int kmax = min((j0 + 1) / 4, (mfit - 1) / 4);
+        n += kmax + 2;
+    }
+    return n;
+}
+
+__device__ void alpha_jobs(int mfit, int* jobs) {
+    if (threadIdx.x == 0) {
+        const int kB = (mfit + 1) & ~1;
+        int n = 0;
+        for (int j0 = 0; j0 < mfit; j0 += 2) {
+            const int kmax = min((j0 + 1) / 4, (mfit - 1) / 4);
+            for (int kb = 0; kb <= kmax; kb++) jobs[n++] = j0 | ((4 * kb) << 16);
+            jobs[n++] = j0 | (kB << 16);
+        }
+        jobs[n++] = kB | (kB << 16);
+    }
+    __syncthreads();
 }
 
 // slots of the misc area
@@ -351,8 +380,6 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
                                       double* alpha_out, double* beta_out, double* Jt, double* yt) {
     const DevProblem& P = *Pp;
     const Layout L = make_layout(P);
-    const int* ent = (const int*)(sm + L.ent);
-    const int nent = P.mfit * (P.mfit + 1) / 2 + P.mfit + 1;
     const int tid = threadIdx.x;
     const int F = P.F, C = P.C, ma = P.ma, npad = P.npad, mfit = P.mfit;
     double* g = sm + L.g;
@@ -593,16 +620,25 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
         }
         __syncthreads();
     }
-    // alpha = J^T W J, beta = J^T W dy, chi2 (mrqcof.c:106-147), rows in
-    // order.  Tile: Ws[r][j] = (J[r][l_j] sig2i) wght (j < mfit),
-    // Ws[r][mfit] = dy dy sig2i wght; Js[r][k] = J[r][l_k] (k < mfit),
-    // Js[r][mfit] = dy, Js[r][mfit+1] = 1.
+    // alpha = J^T W J, beta = J^T W dy, chi2 (mrqcof.c:106-147), every entry
+    // summing the rows in order.  Tile of kRt rows: Ws[r][j] = (J[r][l_j]
+    // sig2i) wght (j < mfit), Ws[r][jC] = dy dy sig2i wght; Js[r][k] =
+    // J[r][l_k] (k < mfit), Js[r][kB] = dy, Js[r][kB+1] = 1; other columns 0.
+    // Each job is a 2 x 4 block of entries (Ws columns j0, j0+1 against Js
+    // columns k0..k0+3), held in registers across the tiles.
+    const int kB = (mfit + 1) & ~1, jC = kB;
+    const int wst = jC + 2, jst = kB + 4;
     double* Ws = work;
-    double* Js = work + kRt * (mfit + 1);
-    const int wst = mfit + 1, jst = mfit + 2;
-    double acc2[kMaxEpt];
+    double* Js = work + kRt * wst;
+    const int* jobs = (const int*)(sm + L.ent);
+    const int njob = alpha_job_count(mfit);
+    double acc2[kJobs][2][4];
 #pragma unroll
-    for (int s = 0; s < kMaxEpt; s++) acc2[s] = 0;
+    for (int q = 0; q < kJobs; q++)
+#pragma unroll
+        for (int a2 = 0; a2 < 2; a2++)
+#pragma unroll
+            for (int b4 = 0; b4 < 4; b4++) acc2[q][a2][b4] = 0;
     for (int r0 = 0; r0 < P.n_rows; r0 += kRt) {
         const int nr = min(kRt, P.n_rows - r0);
         __syncthreads();
@@ -616,37 +652,52 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
         for (int r = tid; r < nr; r += kThreads) {
             const int row = r0 + r;
             const double dy = P.yobs[row] - yt[row];
-            Js[r * jst + mfit] = dy;
-            Js[r * jst + mfit + 1] = 1.0;
-            Ws[r * wst + mfit] = dy * dy * P.sig2i[row] * P.wght[row];
+            for (int k = mfit; k < jst; k++) Js[r * jst + k] = k == kB ? dy : (k == kB + 1 ? 1.0 : 0.0);
+            for (int j = mfit; j < wst; j++) Ws[r * wst + j] = j == jC ? dy * dy * P.sig2i[row] * P.wght[row] : 0.0;
         }
         __syncthreads();
 #pragma unroll
-        for (int s = 0; s < kMaxEpt; s++) {
-            const int e = tid + s * kThreads;
-            if (e < nent) {
-                const int pk = ent[e];
-                const double* w = Ws + (pk & 0xffff);
-                const double* jj = Js + (pk >> 16);
-                double acc = acc2[s];
-                for (int r = 0; r < nr; r++) acc = acc + w[r * wst] * jj[r * jst];
-                acc2[s] = acc;
+        for (int q = 0; q < kJobs; q++) {
+            const int e = tid + q * kThreads;
+            if (e < njob) {
+                const int j0 = jobs[e] & 0xffff, k0 = jobs[e] >> 16;
+                const double* wp = Ws + j0;
+                const double* jp = Js + k0;
+                for (int r = 0; r < nr; r++) {
+                    const double2 w = *reinterpret_cast<const double2*>(wp + r * wst);
+                    const double2 ja = *reinterpret_cast<const double2*>(jp + r * jst);
+                    const double2 jb = *reinterpret_cast<const double2*>(jp + r * jst + 2);
+                    const double wv[2] = {w.x, w.y}, jv[4] = {ja.x, ja.y, jb.x, jb.y};
+#pragma unroll
+                    for (int a2 = 0; a2 < 2; a2++)
+#pragma unroll
+                        for (int b4 = 0; b4 < 4; b4++) acc2[q][a2][b4] = acc2[q][a2][b4] + wv[a2] * jv[b4];
+                }
             }
         }
     }
 #pragma unroll
-    for (int s = 0; s < kMaxEpt; s++) {
-        const int e = tid + s * kThreads;
-        if (e < nent) {
-            const int j = ent[e] & 0xffff, k = ent[e] >> 16;
-            if (k < mfit) {
-                alpha_out[j * mfit + k] = acc2[s];
-                alpha_out[k * mfit + j] = acc2[s];
-            } else if (j < mfit) {
-                beta_out[j] = acc2[s];
-            } else {
-                misc[M_CHISQ] = acc2[s];
-            }
+    for (int q = 0; q < kJobs; q++) {
+        const int e = tid + q * kThreads;
+        if (e < njob) {
+            const int j0 = jobs[e] & 0xffff, k0 = jobs[e] >> 16;
+#pragma unroll
+            for (int a2 = 0; a2 < 2; a2++)
+#pragma unroll
+                for (int b4 = 0; b4 < 4; b4++) {
+                    const int j = j0 + a2, k = k0 + b4;
+                    const double v = acc2[q][a2][b4];
+                    if (j < mfit && k < mfit) {
+                        if (k <= j) {
+                            alpha_out[j * mfit + k] = v;
+                            alpha_out[k * mfit + j] = v;
+                        }
+                    } else if (j < mfit && k == kB) {
+                        beta_out[j] = v;
+                    } else if (j == jC && k == kB + 1) {
+                        misc[M_CHISQ] = v;
+                    }
+                }
         }
     }
     __syncthreads();
@@ -690,11 +741,10 @@ __global__ void __launch_bounds__(kThreads, kFast ? 2 : 1) fit_kernel(const DevP
         double* cg = sm + L.cg;
         double* atry = sm + L.atry;
         double* misc = sm + L.misc;
-        int* ipiv = (int*)(sm + L.ipiv);
         double* Jt = Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride;
         double* yt = Jt + (size_t)ma * P.npad;
         if (mfit != cur_mfit || L.ent != cur_ent) {
-            entry_map(mfit, (int*)(sm + L.ent));
+            alpha_jobs(mfit, (int*)(sm + L.ent));
             cur_mfit = mfit;
             cur_ent = L.ent;
         }
@@ -762,7 +812,7 @@ __global__ void __launch_bounds__(kThreads, kFast ? 2 : 1) fit_kernel(const DevP
             }
             for (int j = tid; j < mfit; j += kThreads) da[j] = beta[j];
             __syncthreads();
-            const int err = gauss_jordan(covar, da, mfit, ipiv, sm + L.work, sm + L.red);
+            const int err = gauss_jordan<NCB + 8>(covar, da, mfit, sm + L.work);
             __syncthreads();
             if (err == 0) {
                 for (int j = tid; j < mfit; j += kThreads) {
@@ -841,7 +891,7 @@ __global__ void __launch_bounds__(kThreads, 1) eval_kernel(const DevProblem* __r
     double* cg = sm + L.cg;
     double* Jt = E.scratch;
     double* yt = Jt + (size_t)P.ma * P.npad;
-    entry_map(P.mfit, (int*)(sm + L.ent));
+    alpha_jobs(P.mfit, (int*)(sm + L.ent));
     for (int i = tid; i < P.ma; i += kThreads) cg[i] = E.a[i];
     __syncthreads();
     evaluate<NCB, kFast>(Pp, sm, cg, sm + L.alpha, sm + L.beta, Jt, yt);

@@ -139,7 +139,7 @@ int fp64_max_blocks_per_sm(const DevProblem& P, int* threads) {
 }
 
 cudaError_t launch_fp64_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s) {
-    if (P.nq <= 0 || P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 > fitimpl::kMaxEpt * fitcommon::kThreads) return cudaErrorInvalidValue;
+    if (P.nq <= 0 || fitimpl::alpha_job_count(P.mfit) > fitimpl::kJobs * fitcommon::kThreads) return cudaErrorInvalidValue;
     switch (P.NCB) {
         case 8: return fitimpl::launch_fits_t<8, false>(P, dP, B, grid, s);
         case 16: return fitimpl::launch_fits_t<16, false>(P, dP, B, grid, s);
@@ -154,7 +154,7 @@ cudaError_t launch_fp64_fits(const DevProblem& P, const DevProblem* dP, const Fi
 }
 
 cudaError_t launch_fp64_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s) {
-    if (P.nq <= 0 || P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 > fitimpl::kMaxEpt * fitcommon::kThreads) return cudaErrorInvalidValue;
+    if (P.nq <= 0 || fitimpl::alpha_job_count(P.mfit) > fitimpl::kJobs * fitcommon::kThreads) return cudaErrorInvalidValue;
     switch (P.NCB) {
         case 8: return fitimpl::launch_eval_t<8, false>(P, dP, E, s);
         case 16: return fitimpl::launch_eval_t<16, false>(P, dP, E, s);

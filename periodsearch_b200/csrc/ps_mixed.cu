@@ -106,7 +106,7 @@ __host__ __device__ inline MLayout make_mlayout(const DevProblem& P) {
     PSB_TAKE(blm, 28)
     PSB_TAKE(misc, 32)
     PSB_TAKE(red, 2 * (kThreads / 32) + 2)
-    PSB_TAKE(gwork, (P.mfit + 2) > 2 * kRtM ? (P.mfit + 2) : 2 * kRtM)
+    PSB_TAKE(gwork, gj_buf_doubles(P.mfit) > 2 * kRtM ? gj_buf_doubles(P.mfit) : 2 * kRtM)
 #undef PSB_TAKE
     o += (uint32_t)d * 8;
     L.flt = o;
@@ -619,7 +619,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
             }
             for (int j = tid; j < mfit; j += kThreads) da[j] = beta[j];
             __syncthreads();
-            const int err = gauss_jordan(covar, da, mfit, ipiv, M.d(L.gwork), M.d(L.red));
+            const int err = gauss_jordan<72>(covar, da, mfit, M.d(L.gwork));
             __syncthreads();
             if (err == 0) {
                 for (int j = tid; j < mfit; j += kThreads) {
