@@ -131,6 +131,60 @@ def cpu_sample(path, conw_r, n_first, fits_per_core=2):
     return done / dt, cores, done, dt
 
 
+REF_EXE = os.path.join(REPO, "oracle", "_ref", "period_search_ref")
+
+
+def ref_cpu_sample(path, n_first, periods_per_proc=1):
+    """Time the reference's own CPU application (oracle/_ref, built from the
+    reference sources) on the host cores: one process per core, each on its
+    own slice of `periods_per_proc` consecutive trial periods (10 fits each)
+    of the same input, started through the reference's checkpoint file
+    (period_search_state = first period - 1).  The convexity-weight line is
+    raised to 10 so that the application skips its pre-pass (it runs while
+    conw_r escl^2 < 10, period_search_BOINC.cpp:489); the fits themselves
+    (points, facets, coefficients, 50 iterations) are unchanged.  Returns
+    (fits/s, cores, fits, seconds) or None when the reference is not built."""
+    if not os.path.exists(REF_EXE):
+        return None
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pso
+
+    o = pso.Oracle(path)
+    o.set_conw_r(o.conw_r)  # sets up the trial-period grid
+    o.refresh()
+    df = o.freq(1) - o.freq(2)
+    lines = open(path).read().split("\n")
+    p_start, coef = lines[0].split()[:2]
+    ia = lines[0].split()[3]
+    cores = os.cpu_count() or 1
+    root = tempfile.mkdtemp(prefix="psref")
+    procs = []
+    for c in range(cores):
+        n0 = n_first + c * periods_per_proc
+        f_end = o.freq(n0) - (periods_per_proc - 0.5) * df
+        d = os.path.join(root, "p%03d" % c)
+        os.makedirs(d)
+        text = list(lines)
+        text[0] = "%s %s %.17g %s" % (p_start, coef, 1.0 / f_end, ia)
+        text[3] = "10\tconvexity weight"
+        open(os.path.join(d, "period_search_in"), "w").write("\n".join(text))
+        open(os.path.join(d, "period_search_state"), "w").write("%d" % (n0 - 1))
+        procs.append(d)
+    t0 = time.perf_counter()
+    running = [subprocess.Popen([REF_EXE], cwd=d, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+               for d in procs]
+    rcs = [p.wait() for p in running]
+    dt = time.perf_counter() - t0
+    done = 0
+    for d, rc in zip(procs, rcs):
+        out = os.path.join(d, "period_search_out")
+        n = len(open(out).read().splitlines()) if os.path.exists(out) else 0
+        if rc != 0 or n != periods_per_proc:
+            raise RuntimeError(f"reference run in {d} ended with {rc}, {n} records")
+        done += 10 * n
+    return done / dt, cores, done, dt
+
+
 def run_reference(args, path, rank):
     if rank != 0:
         return
@@ -138,9 +192,13 @@ def run_reference(args, path, rank):
     import pso
 
     conw_r = pso.Oracle(path).conw_r  # the pre-pass value is not needed for timing a fit
+    kind = "reference" if os.path.exists(REF_EXE) else "port"
     vals = []
     for s in range(args.warmup + args.steps):
-        v, cores, done, dt = cpu_sample(path, conw_r, 1 + 37 * s, fits_per_core=1)
+        if kind == "reference":
+            v, cores, done, dt = ref_cpu_sample(path, 1 + 37 * s)
+        else:
+            v, cores, done, dt = cpu_sample(path, conw_r, 1 + 37 * s, fits_per_core=1)
         if s >= args.warmup:
             vals.append((v, done, dt))
     value = sum(d for _, d, _ in vals) / sum(t for _, _, t in vals)
@@ -148,9 +206,12 @@ def run_reference(args, path, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(t for _, _, t in vals),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": "cpu oracle (reference restated, bit-exact)"},
-        "cpu_baseline": {"value": value, "unit": "fits/s", "cores": cores, "kind": "port",
-                         "sample": f"{cores} processes x 1 fit per step (consecutive periods x poles)"},
+        "config": {"workload": WORKLOAD, "form": "reference CPU application (oracle/_ref, -O3)" if kind == "reference"
+                   else "cpu oracle (reference restated, bit-exact)"},
+        "cpu_baseline": {"value": value, "unit": "fits/s", "cores": cores, "kind": kind,
+                         "sample": (f"{cores} processes x 1 trial period (10 fits) per step, pre-pass skipped"
+                                    if kind == "reference" else
+                                    f"{cores} processes x 1 fit per step (consecutive periods x poles)")},
         "e2e": {"value": value, "unit": "fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -255,7 +316,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--periods-per-step", type=int, default=592)
-    ap.add_argument("--form", default="fp64", choices=["fp64", "fast", "mixed"])
+    ap.add_argument("--form", default="fast", choices=["fp64", "fast", "mixed"],
+                    help="fast: FP64 with the shape block on FP64 tensor cores (the headline); fp64: reference operation order")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--config", default="c2", choices=["c2", "c4"],
@@ -263,10 +325,10 @@ def main():
     ap.add_argument("--asteroids", type=int, default=512)
     ap.add_argument("--c4-periods", type=int, default=4)
     ap.add_argument("--profile", action="store_true",
-                    help="small case for ncu: 14 periods per step, no pre-pass, no e2e/cpu legs")
+                    help="small case for ncu: 30 periods (300 fits, about one wave) per step, no pre-pass, no e2e/cpu legs")
     args = ap.parse_args()
     if args.profile:
-        args.periods_per_step = 14
+        args.periods_per_step = 30
         args.no_cpu = args.no_e2e = True
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -384,15 +446,24 @@ def main():
         peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
     except Exception:
         pass
-    peak = peaks.get("bf16_tflops_sustained")
-    peak_src = "of measured (bf16 sustained)" if peak else "of fallback (1400 TFLOP/s)"
-    peak = peak or 1400.0
+    bf16 = peaks.get("bf16_tflops_sustained")
+    bf16_src = "of measured (bf16 sustained)" if bf16 else "of fallback (1400 TFLOP/s)"
+    bf16 = bf16 or 1400.0
+    # the fits compute in FP64: the bound is the FP64 tensor pipe (equal to the
+    # FP64 SIMT rate on B200), measured live on this GPU
+    fp64_peak = ps.fp64_tensor_peak(local)
     achieved = flop_launch / t_launch / 1e12
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "peak_source": peak_src, "traffic": None,
-                "fp64_nominal_tflops": 37.0, "frac_of_fp64_nominal": achieved / 37.0,
-                "kernel": {"fp64": "fit_kernel<56,false> (FP64 pipe, no FMA by design)", "fast": "fit_kernel<56,true> (FP64 pipe, fused)", "mixed": "mixed_fit_kernel (FP64/FP32 SIMT + tcgen05 shape block)"}[args.form],
-                "flop_per_launch": flop_launch}
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak,
+                "peak_source": "FP64 tensor-core throughput (m8n8k4 MMA) measured live on this GPU; "
+                               "the measured-peaks file holds bf16 and HBM figures only",
+                "traffic": None,
+                "bf16_peak_tflops": bf16, "frac_of_bf16": achieved / bf16, "bf16_peak_source": bf16_src,
+                "kernel": {"fp64": "fit_kernel<56,false> (FP64 SIMT, reference operation order, no FMA)",
+                           "fast": "fit_kernel<56,true> (shape block on FP64 tensor cores, FP64 SIMT per pair)",
+                           "mixed": "mixed_fit_kernel (FP64/FP32 SIMT + tcgen05 split-BF16 shape block)"}[args.form],
+                "flop_per_launch": flop_launch,
+                "flop_rule": "per evaluation 2 N F C + N mfit (mfit + 1), 51 evaluations per fit"}
     line = {
         "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
@@ -409,9 +480,16 @@ def main():
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, cores, done, dt = cpu_sample(path, conw_r, 1)
-        line["cpu_baseline"] = {"value": v, "unit": "fits/s", "cores": cores, "kind": "port",
-                                "sample": f"{done} fits ({cores} processes x 2) of the same workload, {dt:.1f} s"}
+        r = ref_cpu_sample(path, 1)
+        if r is not None:
+            v, cores, done, dt = r
+            line["cpu_baseline"] = {"value": v, "unit": "fits/s", "cores": cores, "kind": "reference",
+                                    "sample": f"{done} fits: {cores} processes of the reference CPU application x 1 "
+                                              f"trial period, pre-pass skipped, {dt:.1f} s"}
+        else:
+            v, cores, done, dt = cpu_sample(path, conw_r, 1)
+            line["cpu_baseline"] = {"value": v, "unit": "fits/s", "cores": cores, "kind": "port",
+                                    "sample": f"{done} fits ({cores} processes x 2) of the same workload, {dt:.1f} s"}
     g.close()
     if dist:
         dist.barrier()

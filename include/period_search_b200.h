@@ -200,6 +200,11 @@ const char* ps_last_error(void);
 /* Kernel launches issued by this process so far (all contexts). */
 long long ps_kernel_launches(void);
 
+/* Measured FP64 tensor-core throughput of `device` in TFLOP/s (m8n8k4 FP64
+ * MMAs from registers on every SM, best of three ~0.1 s runs): the roofline
+ * denominator for the FP64 forms.  No counterpart in the reference. */
+int ps_fp64_tensor_peak(int device, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

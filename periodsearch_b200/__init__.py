@@ -115,6 +115,7 @@ EXPORTS = (
     "ps_scan_device", "ps_fit", "ps_mrqcof", "ps_model", "ps_info", "ps_get_array", "ps_open_host_only",
     "ps_format_record", "ps_last_error", "ps_kernel_launches", "ps_scan_device_noalloc",
     "ps_batch_open", "ps_batch_scan", "ps_batch_scan_device", "ps_batch_fit_cycles", "ps_batch_close",
+    "ps_fp64_tensor_peak",
 )
 
 
@@ -152,6 +153,7 @@ def load_library(path: str | None = None):
         "ps_batch_fit_cycles": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),
         "ps_batch_close": (None, [vp]),
         "ps_kernel_launches": (ctypes.c_longlong, []),
+        "ps_fp64_tensor_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -336,6 +338,13 @@ def _make_desc(d: dict):
     s.ia_par = (ctypes.c_int * 3)(*d["ia_par"])
     keep["_struct"] = s
     return keep, s
+
+
+def fp64_tensor_peak(device: int = 0) -> float:
+    """Measured FP64 tensor-core throughput of the device, TFLOP/s."""
+    v = ctypes.c_double()
+    _check(load_library().ps_fp64_tensor_peak(device, ctypes.byref(v)))
+    return v.value
 
 
 def format_record(rec, first_line: bool = False, conw_line: float = 0.0) -> str:
