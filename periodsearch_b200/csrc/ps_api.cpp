@@ -132,7 +132,7 @@ int upload_static(ps_ctx* c) {
     cudaStream_t s = c->stream;
     const int N = p.n_points, F = p.numfac, C = p.ncoef;
     const int NCB = ((C + 7) / 8) * 8;
-    if (NCB > 64) return fail(PS_ERR_LIMIT, "the FP64 form supports up to 64 shape coefficients (lmax <= 7)");
+    if (NCB > 88) return fail(PS_ERR_LIMIT, "the FP64 forms support up to 88 shape coefficients (lmax <= 8)");
     // points SoA: t, ex, ey, ez, e0x, e0y, e0z, alpha
     std::vector<double> pts((size_t)8 * N);
     for (int i = 0; i < N; i++) {

@@ -26,12 +26,15 @@ int fast_max_blocks_per_sm(const DevProblem& P, int* threads) {
         case 48: return fitimpl::max_blocks_t<48, true>(P);
         case 56: return fitimpl::max_blocks_t<56, true>(P);
         case 64: return fitimpl::max_blocks_t<64, true>(P);
+        case 72: return fitimpl::max_blocks_t<72, true>(P);
+        case 80: return fitimpl::max_blocks_t<80, true>(P);
+        case 88: return fitimpl::max_blocks_t<88, true>(P);
         default: return 0;
     }
 }
 
 cudaError_t launch_fast_fits(const DevProblem& P, const DevProblem* dP, const FitBatch& B, int grid, cudaStream_t s) {
-    if (P.nq <= 0 || fitimpl::alpha_job_count(P.mfit) > fitimpl::kJobs * fitcommon::kThreads) return cudaErrorInvalidValue;
+    if (P.nq <= 0 || P.mfit > P.NCB + 8) return cudaErrorInvalidValue;
     switch (P.NCB) {
         case 8: return fitimpl::launch_fits_t<8, true>(P, dP, B, grid, s);
         case 16: return fitimpl::launch_fits_t<16, true>(P, dP, B, grid, s);
@@ -41,12 +44,15 @@ cudaError_t launch_fast_fits(const DevProblem& P, const DevProblem* dP, const Fi
         case 48: return fitimpl::launch_fits_t<48, true>(P, dP, B, grid, s);
         case 56: return fitimpl::launch_fits_t<56, true>(P, dP, B, grid, s);
         case 64: return fitimpl::launch_fits_t<64, true>(P, dP, B, grid, s);
+        case 72: return fitimpl::launch_fits_t<72, true>(P, dP, B, grid, s);
+        case 80: return fitimpl::launch_fits_t<80, true>(P, dP, B, grid, s);
+        case 88: return fitimpl::launch_fits_t<88, true>(P, dP, B, grid, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 cudaError_t launch_fast_eval(const DevProblem& P, const DevProblem* dP, const EvalOut& E, cudaStream_t s) {
-    if (P.nq <= 0 || fitimpl::alpha_job_count(P.mfit) > fitimpl::kJobs * fitcommon::kThreads) return cudaErrorInvalidValue;
+    if (P.nq <= 0 || P.mfit > P.NCB + 8) return cudaErrorInvalidValue;
     switch (P.NCB) {
         case 8: return fitimpl::launch_eval_t<8, true>(P, dP, E, s);
         case 16: return fitimpl::launch_eval_t<16, true>(P, dP, E, s);
@@ -56,6 +62,9 @@ cudaError_t launch_fast_eval(const DevProblem& P, const DevProblem* dP, const Ev
         case 48: return fitimpl::launch_eval_t<48, true>(P, dP, E, s);
         case 56: return fitimpl::launch_eval_t<56, true>(P, dP, E, s);
         case 64: return fitimpl::launch_eval_t<64, true>(P, dP, E, s);
+        case 72: return fitimpl::launch_eval_t<72, true>(P, dP, E, s);
+        case 80: return fitimpl::launch_eval_t<80, true>(P, dP, E, s);
+        case 88: return fitimpl::launch_eval_t<88, true>(P, dP, E, s);
         default: return cudaErrorInvalidValue;
     }
 }

@@ -125,7 +125,7 @@ struct GjTile {
 };
 
 // gauss_errc.c:9-73 on the n x n row-major matrix a (shared memory,
-// n <= nmax <= 72) with right-hand side b; the solution replaces b, a is left
+// n <= nmax <= 96) with right-hand side b; the solution replaces b, a is left
 // undefined.  Returns 0, 1 or 2, the same value in every thread.  The final
 // column unscrambling of the inverse is omitted: mrqmin (mrqmin.c:59-76) only
 // uses b.
@@ -144,7 +144,7 @@ template <int nmax>
 __device__ int gauss_jordan(double* a, double* b, int n, double* buf) {
     using T = GjTile<nmax>;
     constexpr int kW = T::kW, kR = T::kR, kC = T::kC;
-    static_assert(nmax <= 72 && kR <= 32, "tile");
+    static_assert(nmax <= 96 && kR <= 32 && kC <= 32, "tile");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double* prow = buf;              // pivot row before the step, [n] = b
     double* orow = buf + n + 1;      // row icol before the step, [n] = b

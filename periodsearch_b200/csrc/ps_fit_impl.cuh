@@ -23,8 +23,20 @@ using namespace fitcommon;
 
 constexpr int kFch = 32;     // facets per shared-memory chunk
 constexpr int kRt = 32;      // rows per alpha tile
-constexpr int kJobs = 2;     // alpha/beta/chi2 blocks per thread
 constexpr int kSortSeg = 1024;  // points sorted together by viewing direction
+
+// Blocks of the alpha/beta/chi2 accumulation for mfit free parameters: for
+// each even j0 <= mfit - 1, the 4-column blocks k0 = 4 kb of the lower
+// triangle (k0 <= j0 + 1) and the beta block k0 = kB; then the chi2 block
+// (jC, kB), kB = jC = mfit rounded up to even.  Packed as j0 | k0 << 16.
+__host__ __device__ constexpr int alpha_job_count(int mfit) {
+    int n = 1;
+    for (int j0 = 0; j0 < mfit; j0 += 2) {
+        const int kmax = (j0 + 1) / 4 < (mfit - 1) / 4 ? (j0 + 1) / 4 : (mfit - 1) / 4;
+        n += kmax + 2;
+    }
+    return n;
+}
 
 // Shared-memory layout, offsets in doubles.
 struct Layout {
@@ -64,23 +76,13 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
 #undef PSB_TAKE
     L.ipiv = o;
     L.ent = o + (P.mfit + 2 + 1) / 2;  // int offset counted in doubles
-    const int nent = P.mfit * (P.mfit + 1) / 2 + P.mfit + 1;
-    L.bytes = (size_t)L.ent * sizeof(double) + (size_t)nent * sizeof(int);
+    L.bytes = (size_t)L.ent * sizeof(double) + (size_t)alpha_job_count(P.mfit) * sizeof(int);
     return L;
 }
 
-// Blocks of the alpha/beta/chi2 accumulation for mfit free parameters: for
-// each even j0 <= mfit - 1, the 4-column blocks k0 = 4 kb of the lower
-// triangle (k0 <= j0 + 1) and the beta block k0 = kB; then the chi2 block
-// (jC, kB), kB = jC = mfit rounded up to even.  Packed as j0 | k0 << 16.
-__host__ __device__ inline int alpha_job_count(int mfit) {
-    int n = 1;
-    for (int j0 = 0; j0 < mfit; j0 += 2) {
-        const int kmax = min((j0 + 1) / 4, (mfit - 1) / 4);
-        n += kmax + 2;
-    }
-    return n;
-}
+// alpha/beta/chi2 blocks per thread for mfit <= NCB + 8
+template <int NCB>
+constexpr int kJobsFor = (alpha_job_count(NCB + 8) + kThreads - 1) / kThreads;
 
 __device__ void alpha_jobs(int mfit, int* jobs) {
     if (threadIdx.x == 0) {
@@ -632,6 +634,7 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
     double* Js = work + kRt * wst;
     const int* jobs = (const int*)(sm + L.ent);
     const int njob = alpha_job_count(mfit);
+    constexpr int kJobs = kJobsFor<NCB>;
     double acc2[kJobs][2][4];
 #pragma unroll
     for (int q = 0; q < kJobs; q++)
@@ -704,7 +707,7 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
 }
 
 template <int NCB, bool kFast>
-__global__ void __launch_bounds__(kThreads, kFast ? 2 : 1) fit_kernel(const DevProblem* __restrict__ Parr, FitBatch Bt) {
+__global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_kernel(const DevProblem* __restrict__ Parr, FitBatch Bt) {
     extern __shared__ __align__(16) double sm[];
     __shared__ int s_work, s_ast;
     const int tid = threadIdx.x;
