@@ -195,6 +195,24 @@ int ps_open_host_only(const char* path, ps_ctx** out);
  * Returns the number of characters written (excluding the NUL). */
 int ps_format_record(const ps_record* r, int first_line, double conw_line, char* buf, int buflen);
 
+/* Matrix-free derivatives at parameters a[ma] (the adjoint form).  No
+ * Jacobian is formed: one pass over the (point, facet) pairs evaluates the
+ * model and the forward product, a second (thread per facet) applies J^T,
+ * so a call costs O(N F + F C) instead of the N F C of mrqcof's explicit
+ * dyda rows (mrqcof.c:16-148), with the same relative-lightcurve
+ * normalisation and convexity rows.  FP64, fused arithmetic (the fast form's
+ * rounding); deterministic.
+ *
+ * ps_chi2_grad: *chi2 and beta[mfit] = J^T W (y_obs - y) over the free
+ * parameters, i.e. the chi2 gradient is -2 beta.  Replaces the beta/chisq
+ * half of the reference's mrqcof (mrqcof.c:106-147) for callers that only
+ * need the gradient.
+ * ps_gn_product: out[mfit] = J^T W (J v) for v[mfit] over the free
+ * parameters -- alpha v with alpha from ps_mrqcof, up to rounding.  No
+ * counterpart in the reference (it forms alpha explicitly). */
+int ps_chi2_grad(ps_ctx* ctx, const double* a, double* chi2, double* beta);
+int ps_gn_product(ps_ctx* ctx, const double* a, const double* v, double* out);
+
 /* Message for the last error on the calling thread ("" if none). */
 const char* ps_last_error(void);
 /* Kernel launches issued by this process so far (all contexts). */

@@ -115,7 +115,7 @@ EXPORTS = (
     "ps_scan_device", "ps_fit", "ps_mrqcof", "ps_model", "ps_info", "ps_get_array", "ps_open_host_only",
     "ps_format_record", "ps_last_error", "ps_kernel_launches", "ps_scan_device_noalloc",
     "ps_batch_open", "ps_batch_scan", "ps_batch_scan_device", "ps_batch_fit_cycles", "ps_batch_close",
-    "ps_fp64_tensor_peak",
+    "ps_fp64_tensor_peak", "ps_chi2_grad", "ps_gn_product",
 )
 
 
@@ -154,6 +154,8 @@ def load_library(path: str | None = None):
         "ps_batch_close": (None, [vp]),
         "ps_kernel_launches": (ctypes.c_longlong, []),
         "ps_fp64_tensor_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+        "ps_chi2_grad": (ctypes.c_int, [vp, _D, _D, _D]),
+        "ps_gn_product": (ctypes.c_int, [vp, _D, _D, _D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -252,6 +254,23 @@ class PeriodSearch:
         J = np.zeros((self.n_points + 3, self.ma))
         _check(self._lib.ps_model(self._h, _dptr(a), _dptr(y), _dptr(J)))
         return y, J
+
+    def chi2_grad(self, a):
+        """Matrix-free (chi2, beta) at a; the chi2 gradient over the free
+        parameters is -2 beta."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        beta = np.zeros(self.mfit)
+        x2 = np.zeros(1)
+        _check(self._lib.ps_chi2_grad(self._h, _dptr(a), _dptr(x2), _dptr(beta)))
+        return float(x2[0]), beta
+
+    def gn_product(self, a, v):
+        """Matrix-free J^T W (J v) at a for v over the free parameters."""
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        out = np.zeros(self.mfit)
+        _check(self._lib.ps_gn_product(self._h, _dptr(a), _dptr(v), _dptr(out)))
+        return out
 
     def array(self, name: str) -> np.ndarray:
         size = {"nor": 3 * self.numfac, "darea": self.numfac, "dsph": self.numfac * self.ncoef,

@@ -26,7 +26,7 @@ EXE = os.path.join(HERE, "period_search_b200")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 HOST_FLAGS = ["-Xcompiler", "-O3,-fPIC,-ffp-contract=off", "-std=c++17"]
 
-DEVICE_SOURCES = {"ps_fp64.cu": ["-fmad=false"], "ps_fast.cu": [], "ps_mixed.cu": [], "ps_noalloc.cu": [], "ps_peak.cu": []}
+DEVICE_SOURCES = {"ps_fp64.cu": ["-fmad=false"], "ps_fast.cu": [], "ps_mixed.cu": [], "ps_noalloc.cu": [], "ps_peak.cu": [], "ps_adjoint.cu": []}
 HOST_SOURCES = ["ps_host.cpp", "ps_api.cpp", "ps_batch.cpp"]
 
 

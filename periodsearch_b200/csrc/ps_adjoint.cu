@@ -1,0 +1,415 @@
+// Matrix-free derivatives of the convex-inversion model (PS_FORM_FAST
+// arithmetic, FP64): chi2 and beta = J^T W (y_obs - y) -- the chi2 gradient is
+// -2 beta -- and the Gauss-Newton product J^T W (J v), without forming J.
+//
+// The shape block of J is J_pk = Scale_p sum_f Darea_f s_pf g_f Dsph_fk
+// (bright.c:78-85 with Dg = g Dsph, curv.c:31-35).  Its products with a vector
+// and its transpose need no p x k array:
+//   (J v)_p   = Scale_p sum_f Area_f s_pf z_f,      z = Dsph v        (forward)
+//   (J^T l)_k = sum_f (sum_p l_p Scale_p s_pf) Area_f Dsph_fk       (adjoint)
+// so one product costs two passes over the (point, facet) pairs plus two
+// F x C contractions instead of the N F C of the explicit Jacobian.  The eight
+// non-shape columns are formed per point.  The relative-lightcurve
+// normalisation (mrqcof.c:92-104), J'_r = coef (J_r - y_r dave / ave) with
+// dave = sum_r J_r and J'_r1 = 0, becomes per-lightcurve scalars:
+//   (J' v)_r  = coef ((J v)_r - y_r sum_{r'} (J v)_{r'} / ave)   (v_1 left out)
+//   J'^T u    = J^T l,  l_r = coef (u_r - sum_{r'} y_{r'} u_{r'} / ave).
+// The convexity rows (conv.c:12-29) are added explicitly.  Every reduction
+// runs in a fixed order, so results are deterministic.
+//
+// Kernels, in stream order: adj_setup (1 CTA: blmatrix, curv, z, convexity
+// rows), adj_points (thread per point), adj_rows (1 CTA: normalisation,
+// residuals, chi2, adjoint weights), adj_facets (thread per facet, blocks of
+// points), adj_final (1 CTA: the F x C contraction, non-shape columns).
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "ps_adjoint.hpp"
+#include "ps_device.hpp"
+#include "ps_fit_common.cuh"
+
+namespace psb {
+namespace {
+
+using namespace fitcommon;
+
+constexpr int kPtThreads = 128;  // adj_points: points per CTA
+constexpr int kFacetChunk = 256; // adj_points: facets staged per chunk
+constexpr int kFcThreads = 128;  // adj_facets: facets per CTA
+constexpr int kPtBlock = 512;    // adj_facets: points per CTA (staged)
+
+// misc slots
+enum { X_B = 0, X_D = 9, X_CL = 27, X_CLS = 28, X_OMG = 29, X_P1 = 30, X_P2 = 31, X_P3 = 32, X_CHK = 33,
+       X_CONVJV = 36, X_N = 40 };
+
+__device__ double block_sum(double v, double* red) {
+    // fixed-order tree: warp shuffles, then warp 0 over the warp partials
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[warp] = v;
+    __syncthreads();
+    double s = 0;
+    if (warp == 0) {
+        s = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) red[0] = s;
+    }
+    __syncthreads();
+    s = red[0];
+    __syncthreads();
+    return s;
+}
+
+__global__ void adj_setup(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    const double* a = W.a;
+    const int tid = threadIdx.x, F = P.F, C = P.C, NCB = P.NCB;
+    double* x = W.misc;
+    if (tid == 0) {
+        blmatrix(a[C], a[C + 1], x + X_B, x + X_D);
+        x[X_CL] = exp(a[C + 6]);
+        x[X_CLS] = a[C + 7];
+        x[X_OMG] = a[C + 2];
+        x[X_P1] = a[C + 3];
+        x[X_P2] = a[C + 4];
+        x[X_P3] = a[C + 5];
+    }
+    // curv.c:15-37, and z = Dsph v, z0 = z without the first coefficient
+    for (int f = tid; f < F; f += blockDim.x) {
+        const double* pl = P.cpl + (size_t)f * P.nq;
+        const double* fc = P.cfc + (size_t)f * (P.mmax + 1);
+        const double* fs = P.cfs + (size_t)f * (P.mmax + 1);
+        double gi = 0;
+        int n = 0, q = 0;
+        for (int m = 0; m <= P.mmax; m++) {
+            for (int l = m; l <= P.lmax; l++) {
+                double fsum = a[n] * fc[m];
+                n++;
+                if (m != 0) {
+                    fsum = fma(a[n], fs[m], fsum);
+                    n++;
+                }
+                gi = fma(pl[q], fsum, gi);
+                q++;
+            }
+        }
+        gi = exp(gi);
+        W.g[f] = gi;
+        W.area[f] = P.fac[(size_t)f * 4 + 3] * gi;
+        double z = 0;
+        const double* ds = P.dsph + (size_t)f * NCB;
+        if (W.v)
+            for (int k = 1; k < C; k++) z = fma(ds[k], W.v[k], z);
+        W.z0[f] = z;
+        W.z[f] = W.v ? fma(ds[0], W.v[0], z) : 0.0;
+    }
+    __syncthreads();
+    // convexity rows: chck_nc = sum Area n_nc, dres_nc,k = sum Darea g Dsph_k n_nc
+    for (int job = tid; job < 3 + 3 * C; job += blockDim.x) {
+        double s = 0;
+        if (job < 3) {
+            for (int f = 0; f < F; f++) s = fma(W.area[f], P.fac[(size_t)f * 4 + job], s);
+            x[X_CHK + job] = s;
+        } else {
+            const int nc = (job - 3) / C, k = (job - 3) - nc * C;
+            for (int f = 0; f < F; f++)
+                s = fma(W.area[f] * P.dsph[(size_t)f * NCB + k], P.fac[(size_t)f * 4 + nc], s);
+            W.dres[nc * C + k] = s;
+        }
+    }
+    __syncthreads();
+    if (tid < 3) {
+        double s = 0;
+        if (W.v)
+            for (int k = 0; k < C; k++) s = fma(W.dres[tid * C + k], W.v[k], s);
+        x[X_CONVJV + tid] = s;
+    }
+}
+
+// Per point: the model, the eight non-shape columns of J, the shape part of
+// J v (with and without the first coefficient), Scale, and e, e0 for the
+// adjoint pass.
+__global__ void __launch_bounds__(kPtThreads) adj_points(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    __shared__ double sf[6][kFacetChunk];  // nx, ny, nz, Area, z, z0
+    const int tid = threadIdx.x, F = P.F, C = P.C;
+    const int p = blockIdx.x * kPtThreads + tid;
+    const bool act = p < P.n_points;
+    const double* x = W.misc;
+    const double cl = x[X_CL], cls = x[X_CLS];
+    PointGeom G;
+    if (act) point_geometry(P, p, x + X_B, x + X_D, x[X_OMG], x[X_P1], x[X_P2], x[X_P3], G);
+    double br = 0, sz = 0, sz0 = 0, s_cl = 0, s_cls = 0;
+    double T0 = 0, T1 = 0, T2 = 0, S0 = 0, S1 = 0, S2 = 0;
+    for (int f0 = 0; f0 < F; f0 += kFacetChunk) {
+        const int nf = min(kFacetChunk, F - f0);
+        __syncthreads();
+        for (int i = tid; i < nf; i += kPtThreads) {
+            const double* fa = P.fac + (size_t)(f0 + i) * 4;
+            sf[0][i] = fa[0];
+            sf[1][i] = fa[1];
+            sf[2][i] = fa[2];
+            sf[3][i] = W.area[f0 + i];
+            sf[4][i] = W.z[f0 + i];
+            sf[5][i] = W.z0[f0 + i];
+        }
+        __syncthreads();
+        if (!act) continue;
+        for (int i = 0; i < nf; i++) {
+            const double nx = sf[0][i], ny = sf[1][i], nz = sf[2][i];
+            const double mu = G.e[0] * nx + G.e[1] * ny + G.e[2] * nz;
+            const double mu0 = G.e0[0] * nx + G.e0[1] * ny + G.e0[2] * nz;
+            if (mu > kTinyD && mu0 > kTinyD) {
+                const double ar = sf[3][i];
+                const double r = 1.0 / (mu + mu0);
+                const double s = mu * mu0 * fma(cls, r, cl);
+                const double t = ar * s;
+                br += t;
+                sz = fma(t, sf[4][i], sz);
+                sz0 = fma(t, sf[5][i], sz0);
+                const double q0 = mu0 * r, q1 = mu * r;
+                const double w = ar * fma(cls * q0, q0, cl * mu0);
+                const double w0 = ar * fma(cls * q1, q1, cl * mu);
+                T0 = fma(w, nx, T0);
+                T1 = fma(w, ny, T1);
+                T2 = fma(w, nz, T2);
+                S0 = fma(w0, nx, S0);
+                S1 = fma(w0, ny, S1);
+                S2 = fma(w0, nz, S2);
+                const double mm = mu * mu0 * ar;
+                s_cl += mm;
+                s_cls = fma(mm, r, s_cls);
+            }
+        }
+    }
+    if (!act) return;
+    const double sc = G.scale;
+    double jn[8];
+    const double T[3] = {T0, T1, T2}, S[3] = {S0, S1, S2};
+    for (int k = 0; k < 3; k++) {
+        double v = 0;
+        for (int j = 0; j < 3; j++) v = fma(T[j], G.de[j][k], fma(S[j], G.de0[j][k], v));
+        jn[k] = sc * v;
+    }
+    jn[3] = br * G.dphp[0];
+    jn[4] = br * G.dphp[1];
+    jn[5] = br * G.dphp[2];
+    jn[6] = sc * s_cl * cl;
+    jn[7] = sc * s_cls;
+    double ns = 0;
+    for (int j = 0; j < 8; j++) {
+        W.jns[(size_t)j * P.n_points + p] = jn[j];
+        if (W.v) ns = fma(jn[j], W.v[C + j], ns);
+    }
+    W.y[p] = br * sc;
+    W.scale[p] = sc;
+    W.jv[p] = fma(sc, sz, ns);
+    W.jv0[p] = fma(sc, sz0, ns);
+    for (int c = 0; c < 3; c++) {
+        W.e6[(size_t)c * P.n_points + p] = G.e[c];
+        W.e6[(size_t)(3 + c) * P.n_points + p] = G.e0[c];
+    }
+}
+
+// Normalisation, residuals, chi2 and the adjoint weights; one CTA.
+__global__ void adj_rows(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    __shared__ double red[32];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int nlc = P.n_lc - 1;  // the last lightcurve is the convexity pseudo-curve
+    double* lc_ave = W.lcw;
+    double* lc_s = W.lcw + nlc;
+    double* lc_k = W.lcw + 2 * nlc;
+    double* lc_coef = W.lcw + 3 * nlc;
+    // per relative lightcurve: ave = sum y, S = sum (J v without v_1)
+    for (int lc = 0; lc < nlc; lc++) {
+        if (!P.lc_rel[lc]) continue;
+        const int r0 = P.lc_start[lc], r1 = P.lc_start[lc + 1];
+        double sy = 0, sj = 0;
+        for (int r = r0 + tid; r < r1; r += nt) {
+            sy += W.y[r];
+            sj += W.jv0[r];
+        }
+        sy = block_sum(sy, red);
+        sj = block_sum(sj, red);
+        if (tid == 0) {
+            lc_ave[lc] = sy;
+            lc_s[lc] = sj;
+            lc_coef[lc] = P.sig[r0] * (double)P.lc_npts[lc] / sy;
+        }
+    }
+    __syncthreads();
+    // rows: normalised model and J v, residual, u
+    double x2 = 0;
+    for (int r = tid; r < P.n_rows; r += nt) {
+        double yy, jv;
+        if (r < P.n_points) {
+            int lc = 0;
+            while (P.lc_start[lc + 1] <= r) lc++;
+            if (P.lc_rel[lc]) {
+                const double coef = lc_coef[lc];
+                yy = coef * W.y[r];
+                jv = coef * (W.jv0[r] - W.y[r] * lc_s[lc] / lc_ave[lc]);
+            } else {
+                yy = W.y[r];
+                jv = W.jv[r];
+            }
+        } else {
+            yy = W.misc[X_CHK + (r - P.n_points)];
+            jv = W.misc[X_CONVJV + (r - P.n_points)];
+        }
+        const double w = P.sig2i[r] * P.wght[r];
+        const double dy = P.yobs[r] - yy;
+        x2 = fma(dy * dy, w, x2);
+        W.u[r] = W.v ? w * jv : w * dy;
+    }
+    x2 = block_sum(x2, red);
+    if (tid == 0) *W.chi2 = x2;
+    // per relative lightcurve: kappa = sum y u / ave
+    for (int lc = 0; lc < nlc; lc++) {
+        if (!P.lc_rel[lc]) continue;
+        const int r0 = P.lc_start[lc], r1 = P.lc_start[lc + 1];
+        double s = 0;
+        for (int r = r0 + tid; r < r1; r += nt) s = fma(W.y[r], W.u[r], s);
+        s = block_sum(s, red);
+        if (tid == 0) lc_k[lc] = s / lc_ave[lc];
+    }
+    __syncthreads();
+    // adjoint weights per point: l (all columns), l0 (the first shape
+    // coefficient, zero on relative rows); ls = l Scale for the facet pass
+    for (int r = tid; r < P.n_points; r += nt) {
+        int lc = 0;
+        while (P.lc_start[lc + 1] <= r) lc++;
+        double l = W.u[r], l0 = l;
+        if (P.lc_rel[lc]) {
+            l = lc_coef[lc] * (W.u[r] - lc_k[lc]);
+            l0 = 0.0;
+        }
+        W.lam[r] = l;
+        W.ls[r] = l * W.scale[r];
+        W.ls0[r] = l0 * W.scale[r];
+    }
+}
+
+// q_f = sum_p ls_p s_pf and q0_f = sum_p ls0_p s_pf over a block of points;
+// thread per facet, points staged in shared memory.
+__global__ void __launch_bounds__(kFcThreads) adj_facets(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    __shared__ double sp[8][kPtBlock];  // e (3), e0 (3), ls, ls0
+    const int f = blockIdx.x * kFcThreads + threadIdx.x;
+    const int p0 = blockIdx.y * kPtBlock;
+    const int np = min(kPtBlock, P.n_points - p0);
+    for (int i = threadIdx.x; i < np; i += kFcThreads) {
+        for (int c = 0; c < 6; c++) sp[c][i] = W.e6[(size_t)c * P.n_points + p0 + i];
+        sp[6][i] = W.ls[p0 + i];
+        sp[7][i] = W.ls0[p0 + i];
+    }
+    __syncthreads();
+    if (f >= P.F) return;
+    const double cl = W.misc[X_CL], cls = W.misc[X_CLS];
+    const double nx = P.fac[(size_t)f * 4 + 0], ny = P.fac[(size_t)f * 4 + 1], nz = P.fac[(size_t)f * 4 + 2];
+    double q = 0, q0 = 0;
+    for (int i = 0; i < np; i++) {
+        const double mu = sp[0][i] * nx + sp[1][i] * ny + sp[2][i] * nz;
+        const double mu0 = sp[3][i] * nx + sp[4][i] * ny + sp[5][i] * nz;
+        if (mu > kTinyD && mu0 > kTinyD) {
+            const double r = 1.0 / (mu + mu0);
+            const double s = mu * mu0 * fma(cls, r, cl);
+            q = fma(sp[6][i], s, q);
+            q0 = fma(sp[7][i], s, q0);
+        }
+    }
+    W.q[(size_t)blockIdx.y * P.F + f] = q;
+    W.q0[(size_t)blockIdx.y * P.F + f] = q0;
+}
+
+// out_k = sum_f Q_f Area_f Dsph_fk (Q0 for the first coefficient) + the
+// convexity rows; out_{C+j} = sum_p l_p J_p,C+j; then the free parameters.
+__global__ void adj_final(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    __shared__ double red[32];
+    const int tid = threadIdx.x, nt = blockDim.x, F = P.F, C = P.C;
+    for (int f = tid; f < F; f += nt) {
+        double s = 0, s0 = 0;
+        for (int b = 0; b < W.npb; b++) {
+            s += W.q[(size_t)b * F + f];
+            s0 += W.q0[(size_t)b * F + f];
+        }
+        W.qs[f] = s * W.area[f];
+        W.qs0[f] = s0 * W.area[f];
+    }
+    __syncthreads();
+    for (int k = tid; k < C; k += nt) {
+        const double* q = k == 0 ? W.qs0 : W.qs;
+        double s = 0;
+        for (int f = 0; f < F; f++) s = fma(q[f], P.dsph[(size_t)f * P.NCB + k], s);
+        for (int nc = 0; nc < 3; nc++) s = fma(W.dres[nc * C + k], W.u[P.n_points + nc], s);
+        W.full[k] = s;
+    }
+    for (int j = 0; j < 8; j++) {
+        double s = 0;
+        for (int p = tid; p < P.n_points; p += nt) s = fma(W.lam[p], W.jns[(size_t)j * P.n_points + p], s);
+        s = block_sum(s, red);
+        if (tid == 0) W.full[C + j] = s;
+    }
+    __syncthreads();
+    for (int i = tid; i < P.mfit; i += nt) W.out[i] = W.full[P.free_idx[i]];
+}
+
+}  // namespace
+
+size_t adjoint_work_doubles(const DevProblem& P) {
+    const size_t N = P.n_points, F = P.F;
+    const size_t npb = (N + kPtBlock - 1) / kPtBlock;
+    return 2 * (size_t)P.ma + F * 7 + 3 * (size_t)P.C + X_N + N * (8 + 6 + 7) + P.n_rows + 4 * (size_t)P.n_lc +
+           2 * npb * F + 2 * (size_t)P.ma + 8;
+}
+
+cudaError_t launch_adjoint(const DevProblem& P, const DevProblem* dP, double* work, const double* d_a,
+                           const double* d_v, double* d_out, double* d_chi2, cudaStream_t s) {
+    AdjWork W{};
+    const size_t N = P.n_points, F = P.F;
+    W.npb = (int)((N + kPtBlock - 1) / kPtBlock);
+    double* o = work;
+    auto take = [&](size_t n) {
+        double* r = o;
+        o += n;
+        return r;
+    };
+    W.a = d_a;
+    W.v = d_v;
+    W.g = take(F);
+    W.area = take(F);
+    W.z = take(F);
+    W.z0 = take(F);
+    W.qs = take(F);
+    W.qs0 = take(F);
+    take(F);
+    W.dres = take(3 * (size_t)P.C);
+    W.misc = take(X_N);
+    W.y = take(N);
+    W.scale = take(N);
+    W.jv = take(N);
+    W.jv0 = take(N);
+    W.lam = take(N);
+    W.ls = take(N);
+    W.ls0 = take(N);
+    W.jns = take(8 * N);
+    W.e6 = take(6 * N);
+    W.u = take(P.n_rows);
+    W.lcw = take(4 * (size_t)P.n_lc);
+    W.q = take((size_t)W.npb * F);
+    W.q0 = take((size_t)W.npb * F);
+    W.full = take(P.ma + 8);
+    W.out = d_out;
+    W.chi2 = d_chi2;
+    adj_setup<<<1, 256, 0, s>>>(dP, W);
+    adj_points<<<(unsigned)((N + kPtThreads - 1) / kPtThreads), kPtThreads, 0, s>>>(dP, W);
+    adj_rows<<<1, 256, 0, s>>>(dP, W);
+    adj_facets<<<dim3((unsigned)((F + kFcThreads - 1) / kFcThreads), (unsigned)W.npb), kFcThreads, 0, s>>>(dP, W);
+    adj_final<<<1, 256, 0, s>>>(dP, W);
+    return cudaGetLastError();
+}
+
+}  // namespace psb

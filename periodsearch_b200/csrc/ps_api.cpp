@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/period_search_b200.h"
+#include "ps_adjoint.hpp"
 #include "ps_ctx.hpp"
 #include "ps_device.hpp"
 #include "ps_host.hpp"
@@ -492,6 +493,7 @@ void ps_close(ps_ctx* c) {
         c->d_fits.release();
         c->d_rec.release();
         c->d_eval.release();
+        c->d_adj.release();
         c->d_dp.release();
         c->d_fac32.release();
         c->d_bsw.release();
@@ -653,6 +655,47 @@ int ps_mrqcof(ps_ctx* c, const double* a, double* alpha, double* beta, double* c
     if (beta) std::memcpy(beta, be.data(), be.size() * sizeof(double));
     if (chisq) *chisq = x2;
     return PS_OK;
+}
+
+// Matrix-free chi2 / beta (v == nullptr) or Gauss-Newton product (v over
+// the mfit free parameters) at parameters a.
+static int run_adjoint(ps_ctx* c, const double* a, const double* v, double* chi2, double* out) {
+    int rc = check_ready(c, true);
+    if (rc) return rc;
+    if (!a) return fail(PS_ERR_ARG, "null parameter vector");
+    PSB_CUDA(cudaSetDevice(c->device));
+    const psb::DevProblem& d = c->dp;
+    const size_t work = psb::adjoint_work_doubles(d);
+    PSB_CUDA(c->d_adj.ensure(work + 2 * (size_t)d.ma + d.mfit + 2));
+    double* d_work = c->d_adj.p;
+    double* d_a = d_work + work;
+    double* d_v = d_a + d.ma;
+    double* d_out = d_v + d.ma;
+    double* d_chi2 = d_out + d.mfit;
+    PSB_CUDA(cudaMemcpyAsync(d_a, a, d.ma * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (v) {
+        std::vector<double> vf(d.ma, 0.0);
+        for (int i = 0; i < d.mfit; i++) vf[c->free_idx[i]] = v[i];
+        PSB_CUDA(cudaMemcpyAsync(d_v, vf.data(), d.ma * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PSB_CUDA(cudaStreamSynchronize(c->stream));  // vf leaves scope
+    }
+    PSB_CUDA(psb::launch_adjoint(d, c->d_dp.p, d_work, d_a, v ? d_v : nullptr, d_out, d_chi2, c->stream));
+    for (int k = 0; k < 5; k++) psb::count_launch();
+    double x2 = 0;
+    if (out) PSB_CUDA(cudaMemcpyAsync(out, d_out, d.mfit * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PSB_CUDA(cudaMemcpyAsync(&x2, d_chi2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PSB_CUDA(cudaStreamSynchronize(c->stream));
+    if (chi2) *chi2 = x2;
+    return PS_OK;
+}
+
+int ps_chi2_grad(ps_ctx* c, const double* a, double* chi2, double* beta) {
+    return run_adjoint(c, a, nullptr, chi2, beta);
+}
+
+int ps_gn_product(ps_ctx* c, const double* a, const double* v, double* out) {
+    if (!v) return fail(PS_ERR_ARG, "null direction vector");
+    return run_adjoint(c, a, v, nullptr, out);
 }
 
 int ps_model(ps_ctx* c, const double* a, double* ymod, double* dyda) {

@@ -62,6 +62,7 @@ struct ps_ctx {
     psb::DevBuf<psb::FitOut> d_fits;
     psb::DevBuf<ps_record> d_rec;
     psb::DevBuf<double> d_eval;
+    psb::DevBuf<double> d_adj;  // matrix-free work arrays
     psb::DevBuf<psb::DevProblem> d_dp;
     psb::DevBuf<float> d_fac32;
     psb::DevBuf<uint16_t> d_bsw;
