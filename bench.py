@@ -40,9 +40,17 @@ WORKLOAD = ("c2 production sparse search: N=760 (600 sparse + 2x80 dense), lmax=
             "50 LM iterations/fit, 2-100 h at step coef 2.15 (39153 periods) x 10 poles")
 
 
-def make_input(directory: str) -> str:
+WORKLOAD_C5 = ("c5 large shape: N=20000 (40x100 dense + 16000 sparse), true lmax=10, fit lmax=mmax=8 (C=81), "
+               "nrows=16 (F=2048), 50 LM iterations/fit, 2000 trial periods x 10 poles; explicit J in HBM")
+
+
+def make_input(directory: str, config: str = "c2") -> str:
     from periodsearch_b200 import synth
 
+    if config == "c5":
+        w = synth.make_workload("c5_lmax8_n20000_f2048", 5, dense_lcs=40, dense_pts=100, sparse_pts=16000,
+                                years=10, true_lmax=10, fit_lmax=8, nrows=16, noise=0.03, n_periods=2000)
+        return synth.write_input(w, directory)
     w = synth._c2()
     return synth.write_input(w, directory)
 
@@ -320,13 +328,17 @@ def main():
                     help="fast: FP64 with the shape block on FP64 tensor cores (the headline); fp64: reference operation order")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--config", default="c2", choices=["c2", "c4"],
-                    help="c2: production sparse search (the headline); c4: uneven multi-asteroid batch")
+    ap.add_argument("--config", default="c2", choices=["c2", "c4", "c5"],
+                    help="c2: production sparse search (the headline); c4: uneven multi-asteroid batch; "
+                         "c5: lmax 8 / 2048 facets / 20000 points (14 periods per step, no pre-pass)")
     ap.add_argument("--asteroids", type=int, default=512)
     ap.add_argument("--c4-periods", type=int, default=4)
     ap.add_argument("--profile", action="store_true",
                     help="small case for ncu: 30 periods (300 fits, about one wave) per step, no pre-pass, no e2e/cpu legs")
     args = ap.parse_args()
+    if args.config == "c5":
+        # 140 fits: one wave at one fit (CTA) per SM; the pre-pass is skipped
+        args.periods_per_step = min(args.periods_per_step, 14)
     if args.profile:
         args.periods_per_step = 30
         args.no_cpu = args.no_e2e = True
@@ -340,7 +352,7 @@ def main():
         run_c4(args, local)
         return
     workdir = tempfile.mkdtemp(prefix="psbench")
-    path = make_input(workdir)
+    path = make_input(workdir, args.config)
 
     if args.impl == "reference":
         run_reference(args, path, rank)
@@ -368,7 +380,7 @@ def main():
     # convexity-weight pre-pass (100 fits per round), timed on its own
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    if args.profile:
+    if args.profile or args.config == "c5":
         conw_r = g.conw_r
         g.set_conw_r(conw_r)
     else:
@@ -459,8 +471,8 @@ def main():
                                "the measured-peaks file holds bf16 and HBM figures only",
                 "traffic": None,
                 "bf16_peak_tflops": bf16, "frac_of_bf16": achieved / bf16, "bf16_peak_source": bf16_src,
-                "kernel": {"fp64": "fit_kernel<56,false> (FP64 SIMT, reference operation order, no FMA)",
-                           "fast": "fit_kernel<56,true> (shape block on FP64 tensor cores, FP64 SIMT per pair)",
+                "kernel": {"fp64": f"fit_kernel<{g.ncb},false> (FP64 SIMT, reference operation order, no FMA)",
+                           "fast": f"fit_kernel<{g.ncb},true> (shape block on FP64 tensor cores, FP64 SIMT per pair)",
                            "mixed": "mixed_fit_kernel (FP64/FP32 SIMT + tcgen05 split-BF16 shape block)"}[args.form],
                 "flop_per_launch": flop_launch,
                 "flop_rule": "per evaluation 2 N F C + N mfit (mfit + 1), 51 evaluations per fit"}
@@ -469,7 +481,7 @@ def main():
         "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32+bf16x3" if args.form == "mixed" else "f64",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": {"fp64": "fp64 (drop-in, reference operation order)", "fast": "fast fp64 (rearranged, fused; rounding-level differences)", "mixed": "mixed (FP64 model/solve, FP32 derivatives, tcgen05 split-BF16 shape block)"}[args.form], "periods_per_step": B,
+        "config": {"workload": WORKLOAD_C5 if args.config == "c5" else WORKLOAD, "form": {"fp64": "fp64 (drop-in, reference operation order)", "fast": "fast fp64 (rearranged, fused; rounding-level differences)", "mixed": "mixed (FP64 model/solve, FP32 derivatives, tcgen05 split-BF16 shape block)"}[args.form], "periods_per_step": B,
                    "fits_per_step": fits_per_step, "l2": "flushed (256 MB write) between timed steps",
                    "prepass": {"fits": None, "seconds": prepass_s, "conw_r": conw_r},
                    "parallelism": f"period shards x{world}"},

@@ -194,6 +194,7 @@ class PeriodSearch:
         dbls = (ctypes.c_double * 8)()
         lib.ps_info(self._h, ints, dbls)
         (self.n_points, self.n_lc, self.numfac, self.ncoef, self.ma, self.mfit, self.n_periods) = list(ints)[:7]
+        self.ncb = (self.ncoef + 7) // 8 * 8  # shape columns padded to 8 on the device
         self.escl, self.conw_r, self.freq_start, self.freq_end, self.freq_step = list(dbls)[:5]
 
     # -- lifetime
