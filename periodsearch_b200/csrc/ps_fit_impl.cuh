@@ -67,6 +67,8 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     if (2 * kFch * (4 + P.NCB) > chunk) chunk = 2 * kFch * (4 + P.NCB);  // fast form: two staged chunks
     const int kB = (P.mfit + 1) & ~1;
     int tile = kRt * (kB + 2) + kRt * (kB + 4);  // alpha tiles Ws, Js
+    const int st8 = (kB + 2 + 7) / 8 * 8 + 4;     // fast form: 8-column tiles
+    if (2 * kRt * st8 > tile) tile = 2 * kRt * st8;
     int w = chunk > tile ? chunk : tile;
     if (P.mfit + 2 > w) w = P.mfit + 2;
     if (kSortSeg > w) w = kSortSeg;  // sort keys (uint64) before the point loop
@@ -371,6 +373,101 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
     }
 }
 
+// alpha = J^T W J, beta = J^T W dy, chi2 (mrqcof.c:106-147) on the FP64
+// tensor cores (fast form).  Tiles of kRt rows: Ws[r][j] = (J[r][l_j] sig2i)
+// wght (j < mfit), Ws[r][jC] = dy dy sig2i wght; Js[r][k] = J[r][l_k]
+// (k < mfit), Js[r][kB] = dy, Js[r][kB+1] = 1; all other columns up to 8 T and
+// the rows past the end zero.  Output tiles of 8 x 8 entries: the lower
+// triangle (kt <= jt) and the tiles above it in the beta/chi2 column; a warp
+// accumulates its tiles over all rows with m8n8k4 MMAs (A = Ws^T, B = Js).
+template <int NCB>
+__device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* Jt, const double* yt, double* work,
+                                             double* alpha_out, double* beta_out, double* misc) {
+    constexpr int kBmax = (NCB + 8 + 1) & ~1;
+    constexpr int Tmax = (kBmax + 2 + 7) / 8;
+    constexpr int kTiles = (Tmax * (Tmax + 1) / 2 + Tmax + kThreads / 32 - 1) / (kThreads / 32);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
+    const int mfit = P.mfit, npad = P.npad;
+    const int kB = (mfit + 1) & ~1, jC = kB;
+    const int T = (kB + 2 + 7) / 8, st = T * 8 + 4, ktB = kB / 8;
+    const int ntri = T * (T + 1) / 2, ntile = ntri + ktB;
+    double* Ws = work;
+    double* Js = work + kRt * st;
+    int tj[kTiles], tk[kTiles];
+    double acc[kTiles][2];
+#pragma unroll
+    for (int i = 0; i < kTiles; i++) {
+        const int t = warp + i * (kThreads / 32);
+        int jt = 0, kt = 0;
+        if (t < ntri) {
+            while ((jt + 1) * (jt + 2) / 2 <= t) jt++;
+            kt = t - jt * (jt + 1) / 2;
+        } else {
+            jt = t - ntri;
+            kt = ktB;
+        }
+        tj[i] = t < ntile ? jt * 8 : -1;
+        tk[i] = kt * 8;
+        acc[i][0] = acc[i][1] = 0;
+    }
+    for (int r0 = 0; r0 < P.n_rows; r0 += kRt) {
+        const int nr = min(kRt, P.n_rows - r0);
+        const int nr4 = (nr + 3) & ~3;
+        __syncthreads();
+        for (int idx = tid; idx < nr * mfit; idx += kThreads) {
+            const int j = idx / nr, r = idx - j * nr;
+            const int row = r0 + r;
+            const double d = Jt[(size_t)P.free_idx[j] * npad + row];
+            Js[r * st + j] = d;
+            Ws[r * st + j] = d * P.sig2i[row] * P.wght[row];
+        }
+        for (int idx = tid; idx < nr4 * (st - mfit); idx += kThreads) {
+            const int r = idx / (st - mfit), k = mfit + (idx - r * (st - mfit));
+            double jv = 0.0, wv = 0.0;
+            if (r < nr) {
+                const int row = r0 + r;
+                const double dy = P.yobs[row] - yt[row];
+                jv = k == kB ? dy : (k == kB + 1 ? 1.0 : 0.0);
+                wv = k == jC ? dy * dy * P.sig2i[row] * P.wght[row] : 0.0;
+            }
+            Js[r * st + k] = jv;
+            Ws[r * st + k] = wv;
+        }
+        for (int idx = tid; idx < (nr4 - nr) * mfit; idx += kThreads) {
+            const int r = nr + idx / mfit, k = idx - (idx / mfit) * mfit;
+            Js[r * st + k] = 0.0;
+            Ws[r * st + k] = 0.0;
+        }
+        __syncthreads();
+        for (int rr = 0; rr < nr4; rr += 4) {
+            const double* wrow = Ws + (rr + q) * st + g;
+            const double* jrow = Js + (rr + q) * st + g;
+#pragma unroll
+            for (int i = 0; i < kTiles; i++)
+                if (tj[i] >= 0) dmma_8x8x4(acc[i][0], acc[i][1], wrow[tj[i]], jrow[tk[i]]);
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < kTiles; i++) {
+        if (tj[i] < 0) continue;
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int j = tj[i] + g, k = tk[i] + 2 * q + e;
+            const double v = acc[i][e];
+            if (j < mfit && k < mfit) {
+                if (k <= j) {
+                    alpha_out[j * mfit + k] = v;
+                    alpha_out[k * mfit + j] = v;
+                }
+            } else if (j < mfit && k == kB) {
+                beta_out[j] = v;
+            } else if (j == jC && k == kB + 1) {
+                misc[M_CHISQ] = v;
+            }
+        }
+    }
+}
+
 // One model evaluation, the reference's mrqcof (mrqcof.c:16-148) at
 // parameters a (shared memory).  Writes the symmetrised alpha and beta into
 // alpha_out / beta_out (shared memory) and chi2, the convexity residuals
@@ -433,13 +530,16 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
     for (int job = tid; job < 4 + 3 * C; job += kThreads) {
         double s = 0;
         if (job < 3) {
+#pragma unroll 8
             for (int f = 0; f < F; f++) s = s + area[f] * P.fac[(size_t)f * 4 + job];
             misc[M_CHK0 + job] = s;
         } else if (job == 3) {
+#pragma unroll 8
             for (int f = 0; f < F; f++) s = s + area[f];
             misc[M_SAREA] = s;
         } else {
             const int nc = (job - 4) / C, j = (job - 4) - nc * C;
+#pragma unroll 8
             for (int f = 0; f < F; f++) {
                 const double dg = g[f] * P.dsph[(size_t)f * NCB + j];
                 s += P.fac[(size_t)f * 4 + 3] * dg * P.fac[(size_t)f * 4 + nc];
@@ -622,85 +722,89 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
         }
         __syncthreads();
     }
-    // alpha = J^T W J, beta = J^T W dy, chi2 (mrqcof.c:106-147), every entry
-    // summing the rows in order.  Tile of kRt rows: Ws[r][j] = (J[r][l_j]
-    // sig2i) wght (j < mfit), Ws[r][jC] = dy dy sig2i wght; Js[r][k] =
-    // J[r][l_k] (k < mfit), Js[r][kB] = dy, Js[r][kB+1] = 1; other columns 0.
-    // Each job is a 2 x 4 block of entries (Ws columns j0, j0+1 against Js
-    // columns k0..k0+3), held in registers across the tiles.
-    const int kB = (mfit + 1) & ~1, jC = kB;
-    const int wst = jC + 2, jst = kB + 4;
-    double* Ws = work;
-    double* Js = work + kRt * wst;
-    const int* jobs = (const int*)(sm + L.ent);
-    const int njob = alpha_job_count(mfit);
-    constexpr int kJobs = kJobsFor<NCB>;
-    double acc2[kJobs][2][4];
-#pragma unroll
-    for (int q = 0; q < kJobs; q++)
-#pragma unroll
-        for (int a2 = 0; a2 < 2; a2++)
-#pragma unroll
-            for (int b4 = 0; b4 < 4; b4++) acc2[q][a2][b4] = 0;
-    for (int r0 = 0; r0 < P.n_rows; r0 += kRt) {
-        const int nr = min(kRt, P.n_rows - r0);
-        __syncthreads();
-        for (int idx = tid; idx < nr * mfit; idx += kThreads) {
-            const int j = idx / nr, r = idx - j * nr;
-            const int row = r0 + r;
-            const double d = Jt[(size_t)P.free_idx[j] * npad + row];
-            Js[r * jst + j] = d;
-            Ws[r * wst + j] = d * P.sig2i[row] * P.wght[row];
+    if constexpr (kFast) {
+        alpha_tensor<NCB>(P, Jt, yt, work, alpha_out, beta_out, misc);
+    } else {
+        // alpha = J^T W J, beta = J^T W dy, chi2 (mrqcof.c:106-147), every entry
+        // summing the rows in order.  Tile of kRt rows: Ws[r][j] = (J[r][l_j]
+        // sig2i) wght (j < mfit), Ws[r][jC] = dy dy sig2i wght; Js[r][k] =
+        // J[r][l_k] (k < mfit), Js[r][kB] = dy, Js[r][kB+1] = 1; other columns 0.
+        // Each job is a 2 x 4 block of entries (Ws columns j0, j0+1 against Js
+        // columns k0..k0+3), held in registers across the tiles.
+        const int kB = (mfit + 1) & ~1, jC = kB;
+        const int wst = jC + 2, jst = kB + 4;
+        double* Ws = work;
+        double* Js = work + kRt * wst;
+        const int* jobs = (const int*)(sm + L.ent);
+        const int njob = alpha_job_count(mfit);
+        constexpr int kJobs = kJobsFor<NCB>;
+        double acc2[kJobs][2][4];
+    #pragma unroll
+        for (int q = 0; q < kJobs; q++)
+    #pragma unroll
+            for (int a2 = 0; a2 < 2; a2++)
+    #pragma unroll
+                for (int b4 = 0; b4 < 4; b4++) acc2[q][a2][b4] = 0;
+        for (int r0 = 0; r0 < P.n_rows; r0 += kRt) {
+            const int nr = min(kRt, P.n_rows - r0);
+            __syncthreads();
+            for (int idx = tid; idx < nr * mfit; idx += kThreads) {
+                const int j = idx / nr, r = idx - j * nr;
+                const int row = r0 + r;
+                const double d = Jt[(size_t)P.free_idx[j] * npad + row];
+                Js[r * jst + j] = d;
+                Ws[r * wst + j] = d * P.sig2i[row] * P.wght[row];
+            }
+            for (int r = tid; r < nr; r += kThreads) {
+                const int row = r0 + r;
+                const double dy = P.yobs[row] - yt[row];
+                for (int k = mfit; k < jst; k++) Js[r * jst + k] = k == kB ? dy : (k == kB + 1 ? 1.0 : 0.0);
+                for (int j = mfit; j < wst; j++) Ws[r * wst + j] = j == jC ? dy * dy * P.sig2i[row] * P.wght[row] : 0.0;
+            }
+            __syncthreads();
+    #pragma unroll
+            for (int q = 0; q < kJobs; q++) {
+                const int e = tid + q * kThreads;
+                if (e < njob) {
+                    const int j0 = jobs[e] & 0xffff, k0 = jobs[e] >> 16;
+                    const double* wp = Ws + j0;
+                    const double* jp = Js + k0;
+                    for (int r = 0; r < nr; r++) {
+                        const double2 w = *reinterpret_cast<const double2*>(wp + r * wst);
+                        const double2 ja = *reinterpret_cast<const double2*>(jp + r * jst);
+                        const double2 jb = *reinterpret_cast<const double2*>(jp + r * jst + 2);
+                        const double wv[2] = {w.x, w.y}, jv[4] = {ja.x, ja.y, jb.x, jb.y};
+    #pragma unroll
+                        for (int a2 = 0; a2 < 2; a2++)
+    #pragma unroll
+                            for (int b4 = 0; b4 < 4; b4++) acc2[q][a2][b4] = acc2[q][a2][b4] + wv[a2] * jv[b4];
+                    }
+                }
+            }
         }
-        for (int r = tid; r < nr; r += kThreads) {
-            const int row = r0 + r;
-            const double dy = P.yobs[row] - yt[row];
-            for (int k = mfit; k < jst; k++) Js[r * jst + k] = k == kB ? dy : (k == kB + 1 ? 1.0 : 0.0);
-            for (int j = mfit; j < wst; j++) Ws[r * wst + j] = j == jC ? dy * dy * P.sig2i[row] * P.wght[row] : 0.0;
-        }
-        __syncthreads();
-#pragma unroll
+    #pragma unroll
         for (int q = 0; q < kJobs; q++) {
             const int e = tid + q * kThreads;
             if (e < njob) {
                 const int j0 = jobs[e] & 0xffff, k0 = jobs[e] >> 16;
-                const double* wp = Ws + j0;
-                const double* jp = Js + k0;
-                for (int r = 0; r < nr; r++) {
-                    const double2 w = *reinterpret_cast<const double2*>(wp + r * wst);
-                    const double2 ja = *reinterpret_cast<const double2*>(jp + r * jst);
-                    const double2 jb = *reinterpret_cast<const double2*>(jp + r * jst + 2);
-                    const double wv[2] = {w.x, w.y}, jv[4] = {ja.x, ja.y, jb.x, jb.y};
-#pragma unroll
-                    for (int a2 = 0; a2 < 2; a2++)
-#pragma unroll
-                        for (int b4 = 0; b4 < 4; b4++) acc2[q][a2][b4] = acc2[q][a2][b4] + wv[a2] * jv[b4];
-                }
-            }
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < kJobs; q++) {
-        const int e = tid + q * kThreads;
-        if (e < njob) {
-            const int j0 = jobs[e] & 0xffff, k0 = jobs[e] >> 16;
-#pragma unroll
-            for (int a2 = 0; a2 < 2; a2++)
-#pragma unroll
-                for (int b4 = 0; b4 < 4; b4++) {
-                    const int j = j0 + a2, k = k0 + b4;
-                    const double v = acc2[q][a2][b4];
-                    if (j < mfit && k < mfit) {
-                        if (k <= j) {
-                            alpha_out[j * mfit + k] = v;
-                            alpha_out[k * mfit + j] = v;
+    #pragma unroll
+                for (int a2 = 0; a2 < 2; a2++)
+    #pragma unroll
+                    for (int b4 = 0; b4 < 4; b4++) {
+                        const int j = j0 + a2, k = k0 + b4;
+                        const double v = acc2[q][a2][b4];
+                        if (j < mfit && k < mfit) {
+                            if (k <= j) {
+                                alpha_out[j * mfit + k] = v;
+                                alpha_out[k * mfit + j] = v;
+                            }
+                        } else if (j < mfit && k == kB) {
+                            beta_out[j] = v;
+                        } else if (j == jC && k == kB + 1) {
+                            misc[M_CHISQ] = v;
                         }
-                    } else if (j < mfit && k == kB) {
-                        beta_out[j] = v;
-                    } else if (j == jC && k == kB + 1) {
-                        misc[M_CHISQ] = v;
                     }
-                }
+            }
         }
     }
     __syncthreads();
