@@ -67,8 +67,8 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     if (2 * kFch * (4 + P.NCB) > chunk) chunk = 2 * kFch * (4 + P.NCB);  // fast form: two staged chunks
     const int kB = (P.mfit + 1) & ~1;
     int tile = kRt * (kB + 2) + kRt * (kB + 4);  // alpha tiles Ws, Js
-    const int st8 = (kB + 2 + 7) / 8 * 8 + 4;     // fast form: 8-column tiles
-    if (2 * kRt * st8 > tile) tile = 2 * kRt * st8;
+    const int st8 = (kB + 2 + 7) / 8 * 8 + 4;     // fast form: 8-column tiles, two buffers
+    if (2 * kRt * (st8 + 1) > tile) tile = 2 * kRt * (st8 + 1);
     int w = chunk > tile ? chunk : tile;
     if (P.mfit + 2 > w) w = P.mfit + 2;
     if (kSortSeg > w) w = kSortSeg;  // sort keys (uint64) before the point loop
@@ -181,6 +181,10 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -220,8 +224,9 @@ __device__ __forceinline__ void stage_chunk_async(const DevProblem& P, int f0, d
 // the end: the form differs from the reference order by rounding only.
 template <int NCB>
 __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm, const Layout& L, const double* B,
-                                                const double* D, const double* misc, const double* area,
-                                                double* work, double* Jt, double* yt) {
+                                                const double* D, double* misc, const double* g_f,
+                                                const double* area, double* dres, double* work, double* Jt,
+                                                double* yt) {
     constexpr int NT = NCB / 8;                  // accumulator tiles per 8 points
     constexpr int kMT = 1;                       // point tiles per warp
     constexpr int kPts = (kThreads / 32) * 8 * kMT;  // points per pass
@@ -234,6 +239,10 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
     const double cl = misc[M_CL], cls = misc[M_CLS];
     const unsigned full = 0xffffffffu;
     const int nch = (F + kFch - 1) / kFch;
+    constexpr int kSumJobs = (4 + 3 * NCB + kThreads - 1) / kThreads;
+    double fsum[kSumJobs];
+#pragma unroll
+    for (int u = 0; u < kSumJobs; u++) fsum[u] = 0;
     for (int s0 = 0; s0 < P.n_points; s0 += kSortSeg) {
         const int seg = min(kSortSeg, P.n_points - s0);
         __syncthreads();
@@ -279,6 +288,27 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
                 const double* fb = fbuf[ch & 1];
                 const double* db = dbuf[ch & 1];
                 const int nf = min(kFch, F - f0);
+                if (s0 == 0 && base == 0) {
+                    // the facet sums (convexity residuals and derivatives, facet-area
+                    // sum) from the staged chunk, facets in order, one thread per sum
+#pragma unroll
+                    for (int u = 0; u < kSumJobs; u++) {
+                        const int job = tid + u * kThreads;
+                        if (job >= 4 + 3 * C) continue;
+                        double sacc = fsum[u];
+                        if (job < 4) {
+                            for (int ff = 0; ff < nf; ff++)
+                                sacc = sacc + (job < 3 ? area[f0 + ff] * fb[ff * 4 + job] : area[f0 + ff]);
+                        } else {
+                            const int nc = (job - 4) / C, jj = (job - 4) - nc * C;
+                            for (int ff = 0; ff < nf; ff++) {
+                                const double dg = g_f[f0 + ff] * db[ff * NCB + jj];
+                                sacc += fb[ff * 4 + 3] * dg * fb[ff * 4 + nc];
+                            }
+                        }
+                        fsum[u] = sacc;
+                    }
+                }
                 for (int j = 0; j < nf; j += 4) {
                     const int ff = j + q;
                     const bool valid = f0 + ff < F;
@@ -371,15 +401,27 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
             }
         }
     }
+#pragma unroll
+    for (int u = 0; u < kSumJobs; u++) {
+        const int job = tid + u * kThreads;
+        if (job < 3)
+            misc[M_CHK0 + job] = fsum[u];
+        else if (job == 3)
+            misc[M_SAREA] = fsum[u];
+        else if (job < 4 + 3 * C)
+            dres[job - 4] = fsum[u];
+    }
 }
 
 // alpha = J^T W J, beta = J^T W dy, chi2 (mrqcof.c:106-147) on the FP64
-// tensor cores (fast form).  Tiles of kRt rows: Ws[r][j] = (J[r][l_j] sig2i)
-// wght (j < mfit), Ws[r][jC] = dy dy sig2i wght; Js[r][k] = J[r][l_k]
-// (k < mfit), Js[r][kB] = dy, Js[r][kB+1] = 1; all other columns up to 8 T and
-// the rows past the end zero.  Output tiles of 8 x 8 entries: the lower
-// triangle (kt <= jt) and the tiles above it in the beta/chi2 column; a warp
-// accumulates its tiles over all rows with m8n8k4 MMAs (A = Ws^T, B = Js).
+// tensor cores (fast form).  Tiles of kRt rows, two buffers: Js[r][k] =
+// J[r][l_k] (k < mfit), Js[r][kB] = dy, zero elsewhere, and the row weight
+// w[r] = sig2i wght; the next tile's J values arrive by asynchronous copies
+// and its dy and w through registers while the current tile is multiplied.
+// With A = (Js w)^T and B = Js, entry (j, k) is alpha (k <= j < mfit), beta
+// (k = kB) or chi2 (j = k = kB).  Output tiles of 8 x 8 entries: the lower
+// triangle (kt <= jt) and the tiles above it in the beta column; a warp
+// accumulates its tiles over all rows with m8n8k4 MMAs.
 template <int NCB>
 __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* Jt, const double* yt, double* work,
                                              double* alpha_out, double* beta_out, double* misc) {
@@ -387,12 +429,12 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
     constexpr int Tmax = (kBmax + 2 + 7) / 8;
     constexpr int kTiles = (Tmax * (Tmax + 1) / 2 + Tmax + kThreads / 32 - 1) / (kThreads / 32);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, g = lane >> 2, q = lane & 3;
-    const int mfit = P.mfit, npad = P.npad;
-    const int kB = (mfit + 1) & ~1, jC = kB;
+    const int mfit = P.mfit, npad = P.npad, nrows = P.n_rows;
+    const int kB = (mfit + 1) & ~1;
     const int T = (kB + 2 + 7) / 8, st = T * 8 + 4, ktB = kB / 8;
     const int ntri = T * (T + 1) / 2, ntile = ntri + ktB;
-    double* Ws = work;
-    double* Js = work + kRt * st;
+    double* Js[2] = {work, work + kRt * (st + 1)};
+    double* wv[2] = {work + kRt * st, work + kRt * (st + 1) + kRt * st};
     int tj[kTiles], tk[kTiles];
     double acc[kTiles][2];
 #pragma unroll
@@ -410,42 +452,53 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
         tk[i] = kt * 8;
         acc[i][0] = acc[i][1] = 0;
     }
-    for (int r0 = 0; r0 < P.n_rows; r0 += kRt) {
-        const int nr = min(kRt, P.n_rows - r0);
-        const int nr4 = (nr + 3) & ~3;
-        __syncthreads();
+    auto issue = [&](int r0, int b) {
+        const int nr = min(kRt, nrows - r0);
         for (int idx = tid; idx < nr * mfit; idx += kThreads) {
             const int j = idx / nr, r = idx - j * nr;
-            const int row = r0 + r;
-            const double d = Jt[(size_t)P.free_idx[j] * npad + row];
-            Js[r * st + j] = d;
-            Ws[r * st + j] = d * P.sig2i[row] * P.wght[row];
+            cp_async8(Js[b] + r * st + j, Jt + (size_t)P.free_idx[j] * npad + r0 + r);
         }
-        for (int idx = tid; idx < nr4 * (st - mfit); idx += kThreads) {
-            const int r = idx / (st - mfit), k = mfit + (idx - r * (st - mfit));
-            double jv = 0.0, wv = 0.0;
-            if (r < nr) {
-                const int row = r0 + r;
-                const double dy = P.yobs[row] - yt[row];
-                jv = k == kB ? dy : (k == kB + 1 ? 1.0 : 0.0);
-                wv = k == jC ? dy * dy * P.sig2i[row] * P.wght[row] : 0.0;
+        cp_async_commit();
+    };
+    __syncthreads();
+    for (int i = tid; i < 2 * kRt * (st + 1); i += kThreads) work[i] = 0.0;
+    __syncthreads();
+    const int ntl = (nrows + kRt - 1) / kRt;
+    issue(0, 0);
+    if (tid < kRt) {
+        const double dy = tid < nrows ? P.yobs[tid] - yt[tid] : 0.0;
+        Js[0][tid * st + kB] = dy;
+        wv[0][tid] = tid < nrows ? P.sig2i[tid] * P.wght[tid] : 0.0;
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int t = 0; t < ntl; t++) {
+        const int b = t & 1, r0 = t * kRt;
+        const int nr4 = (min(kRt, nrows - r0) + 3) & ~3;
+        double ndy = 0.0, nw = 0.0;
+        if (t + 1 < ntl) {
+            const int r1 = r0 + kRt;
+            issue(r1, b ^ 1);
+            if (tid < kRt && r1 + tid < nrows) {
+                ndy = P.yobs[r1 + tid] - yt[r1 + tid];
+                nw = P.sig2i[r1 + tid] * P.wght[r1 + tid];
             }
-            Js[r * st + k] = jv;
-            Ws[r * st + k] = wv;
         }
-        for (int idx = tid; idx < (nr4 - nr) * mfit; idx += kThreads) {
-            const int r = nr + idx / mfit, k = idx - (idx / mfit) * mfit;
-            Js[r * st + k] = 0.0;
-            Ws[r * st + k] = 0.0;
-        }
-        __syncthreads();
+        const double* jb = Js[b];
+        const double* wb = wv[b];
         for (int rr = 0; rr < nr4; rr += 4) {
-            const double* wrow = Ws + (rr + q) * st + g;
-            const double* jrow = Js + (rr + q) * st + g;
+            const double* row = jb + (rr + q) * st + g;
+            const double w = wb[rr + q];
 #pragma unroll
             for (int i = 0; i < kTiles; i++)
-                if (tj[i] >= 0) dmma_8x8x4(acc[i][0], acc[i][1], wrow[tj[i]], jrow[tk[i]]);
+                if (tj[i] >= 0) dmma_8x8x4(acc[i][0], acc[i][1], row[tj[i]] * w, row[tk[i]]);
         }
+        if (t + 1 < ntl && tid < kRt) {
+            Js[b ^ 1][tid * st + kB] = ndy;
+            wv[b ^ 1][tid] = nw;  // zero past the last row
+        }
+        cp_async_wait_all();
+        __syncthreads();
     }
 #pragma unroll
     for (int i = 0; i < kTiles; i++) {
@@ -461,7 +514,7 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
                 }
             } else if (j < mfit && k == kB) {
                 beta_out[j] = v;
-            } else if (j == jC && k == kB + 1) {
+            } else if (j == kB && k == kB) {
                 misc[M_CHISQ] = v;
             }
         }
@@ -526,7 +579,9 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
     __syncthreads();
     // Sequential facet sums: chck / conv residuals (conv.c:22-27), the
     // facet-area sum (period_search_BOINC.cpp:900-902) and the conv-row shape
-    // derivatives, one thread per sum, facets in order.
+    // derivatives, one thread per sum, facets in order (the fast form forms
+    // them from the facet chunks its point loop stages).
+    if constexpr (!kFast)
     for (int job = tid; job < 4 + 3 * C; job += kThreads) {
         double s = 0;
         if (job < 3) {
@@ -548,7 +603,7 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
         }
     }
     if constexpr (kFast) {
-        point_loop_fast<NCB>(P, sm, L, B, D, misc, area, work, Jt, yt);
+        point_loop_fast<NCB>(P, sm, L, B, D, misc, g, area, dres, work, Jt, yt);
     } else {
         // bright.c:54-125 for every data point, in segments of points sorted by
         // viewing direction
