@@ -177,8 +177,26 @@ int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out) {
     std::vector<psb::DevProblem> probs(n);
     std::vector<double> ndata(n);
     size_t best = 0;
+    // Asteroids on the same facet grid (nrows, lmax, mmax) have identical
+    // facet tables (normals, areas, Dsph, Legendre and Fourier factors);
+    // their fits read one copy, which then stays in L2.
+    std::vector<int> owners;
     for (int a = 0; a < n; a++) {
         probs[a] = ctxs[a]->dp;
+        const psb::Problem& pa = ctxs[a]->prob;
+        for (int o : owners) {
+            const psb::Problem& po = ctxs[o]->prob;
+            if (pa.lmax == po.lmax && pa.mmax == po.mmax && pa.nor == po.nor && pa.darea == po.darea &&
+                pa.dsph == po.dsph && pa.pleg == po.pleg && pa.fc == po.fc && pa.fs == po.fs) {
+                probs[a].fac = ctxs[o]->dp.fac;
+                probs[a].dsph = ctxs[o]->dp.dsph;
+                probs[a].cpl = ctxs[o]->dp.cpl;
+                probs[a].cfc = ctxs[o]->dp.cfc;
+                probs[a].cfs = ctxs[o]->dp.cfs;
+                break;
+            }
+        }
+        if (probs[a].dsph == ctxs[a]->dp.dsph) owners.push_back(a);
         ndata[a] = ctxs[a]->dp.ndata_m3;
         b->stride = std::max(b->stride, (long long)(ctxs[a]->dp.ma + 1) * ctxs[a]->dp.npad);
         const size_t s = smem_of(b, probs[a]);
