@@ -46,10 +46,13 @@ struct ps_batch {
 namespace {
 
 // control block: [0] fits, [1] periods, [2] work counter,
-// [3 .. 3+n] fit offsets, [4+n .. 3+2n] first periods, [4+2n .. 4+3n] period offsets
+// [3 .. 3+n] fit offsets, [4+n .. 3+2n] first periods, [4+2n .. 4+3n] period offsets,
+// [5+3n .. 4+4n] queue order of the asteroids, [5+4n .. 5+5n] queue offsets in that order
 int ctl_fit_off(int) { return 3; }
 int ctl_n_from(int n) { return 4 + n; }
 int ctl_per_off(int n) { return 4 + 2 * n; }
+int ctl_order(int n) { return 5 + 3 * n; }
+int ctl_ord_off(int n) { return 5 + 4 * n; }
 
 #define PSB_BCUDA(call)                                                                      \
     do {                                                                                     \
@@ -85,6 +88,8 @@ int capture(ps_batch* b, size_t fits, size_t periods) {
     fb.n_ast = b->n;
     fb.ast_fit_off = ctl + ctl_fit_off(b->n);
     fb.ast_n_from = ctl + ctl_n_from(b->n);
+    fb.ast_order = ctl + ctl_order(b->n);
+    fb.ast_ord_off = ctl + ctl_ord_off(b->n);
     PSB_BCUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
     cudaError_t e = cudaMemcpyAsync(ctl, b->h_ctl, b->ctl_ints * sizeof(int), cudaMemcpyHostToDevice, b->stream);
     if (e == cudaSuccess)
@@ -128,6 +133,22 @@ int run(ps_batch* b, const int* n_from, const int* n_to, size_t* periods_out, cu
     if (fits > 0x7fffffff) return psb::set_error(PS_ERR_LIMIT, "too many fits in one batch scan");
     h[ctl_fit_off(n) + n] = (int)fits;
     h[ctl_per_off(n) + n] = (int)periods;
+    // longest fits first (cost ~ points x fits), so that the persistent
+    // kernel's last fits are short ones and the SMs finish together
+    std::vector<int> order(n);
+    for (int a = 0; a < n; a++) order[a] = a;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const double cx = (double)b->ctx[x]->prob.n_points * (n_to[x] - n_from[x] + 1);
+        const double cy = (double)b->ctx[y]->prob.n_points * (n_to[y] - n_from[y] + 1);
+        return cx > cy;
+    });
+    int q = 0;
+    for (int k = 0; k < n; k++) {
+        h[ctl_order(n) + k] = order[k];
+        h[ctl_ord_off(n) + k] = q;
+        q += 10 * (n_to[order[k]] - n_from[order[k]] + 1);
+    }
+    h[ctl_ord_off(n) + n] = q;
     h[0] = (int)fits;
     h[1] = (int)periods;
     h[2] = 0;
@@ -210,7 +231,7 @@ int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out) {
                                                : psb::fp64_max_blocks_per_sm(b->head, &threads);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     b->grid = sms * per_sm;
-    b->ctl_ints = (size_t)(5 + 3 * n);
+    b->ctl_ints = (size_t)(6 + 5 * n);
     if (e == cudaSuccess) e = cudaMallocHost(&b->h_ctl, b->ctl_ints * sizeof(int));
     if (e == cudaSuccess) e = b->d_ctl.ensure(b->ctl_ints);
     if (e == cudaSuccess) e = b->d_probs.upload(probs, b->stream);

@@ -68,6 +68,11 @@ struct FitBatch {
     const int* ast_fit_off;
     const int* ast_n_from;
     const int* n_fits_dev;
+    // Optional order of the work queue over the asteroids (n_ast > 1): the
+    // queue hands out the fits of ast_order[0] first, then ast_order[1], ...;
+    // ast_ord_off[k] = queue position of the first fit of ast_order[k].
+    const int* ast_order;
+    const int* ast_ord_off;
 };
 
 // Diagnostics of one evaluation (ps_mrqcof / ps_model): J, y, alpha, beta.

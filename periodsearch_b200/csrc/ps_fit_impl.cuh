@@ -880,15 +880,23 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
             if (w >= nf) {
                 w = -1;
             } else if (Bt.n_ast > 1) {
-                int lo = 0, hi = Bt.n_ast - 1;  // last a with ast_fit_off[a] <= w
+                // queue position -> asteroid; with an order, the queue runs over
+                // the asteroids in that order (largest first) and w becomes the
+                // fit's index in the asteroid-ordered result array
+                const int* off = Bt.ast_order ? Bt.ast_ord_off : Bt.ast_fit_off;
+                int lo = 0, hi = Bt.n_ast - 1;  // last k with off[k] <= w
                 while (lo < hi) {
                     const int mid = (lo + hi + 1) >> 1;
-                    if (Bt.ast_fit_off[mid] <= w)
+                    if (off[mid] <= w)
                         lo = mid;
                     else
                         hi = mid - 1;
                 }
                 a = lo;
+                if (Bt.ast_order) {
+                    a = Bt.ast_order[lo];
+                    w = Bt.ast_fit_off[a] + (w - off[lo]);
+                }
             }
             s_work = w;
             s_ast = a;
