@@ -258,9 +258,13 @@ def run_c4(args, local):
         c = ps.PeriodSearch(p, device=local, form=form)
         c.set_conw_r(c.conw_r)
         ctxs.append(c)
-    batch = ps.PeriodSearchBatch(ctxs)
     P = args.c4_periods
     n_per = np.array([c.n_periods for c in ctxs])
+    tiles = None
+    if not args.no_autotune:
+        a0 = np.ones(len(ctxs), dtype=np.int32)
+        tiles, _ = ps.PeriodSearchBatch.autotune(ctxs, a0, np.minimum(a0 + P - 1, n_per).astype(np.int32))
+    batch = ps.PeriodSearchBatch(ctxs)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     total_periods = int(len(ctxs) * P)
@@ -304,6 +308,10 @@ def run_c4(args, local):
                                f"(mean {np.mean([m for _, m in made]):.0f}), lmax=mmax=6, nrows=10, "
                                f"stop_condition 1e-4 / n_iter_min 5, {P} periods x 10 poles per asteroid per step",
                    "form": args.form, "graph": "persistent fit kernel + reduction replayed from a CUDA graph",
+                   "tiles": ({"fch": tiles[0], "rt": tiles[1], "sortseg": tiles[2],
+                              "chosen_by": "PeriodSearchBatch.autotune (ps_autotune on the work-weighted "
+                                           "median asteroid, checked against the defaults on one batch scan)"}
+                             if tiles else "defaults"),
                    "l2": "flushed (256 MB write) between timed steps"},
         "per_asteroid_ms": {"p50": 1000 * float(np.percentile(per_ast, 50)),
                             "p99": 1000 * float(np.percentile(per_ast, 99)),
@@ -332,6 +340,7 @@ def main():
                     help="c2: production sparse search (the headline); c4: uneven multi-asteroid batch; "
                          "c5: lmax 8 / 2048 facets / 20000 points (14 periods per step, no pre-pass)")
     ap.add_argument("--asteroids", type=int, default=512)
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default tile shapes")
     ap.add_argument("--c4-periods", type=int, default=4)
     ap.add_argument("--profile", action="store_true",
                     help="small case for ncu: 30 periods (300 fits, about one wave) per step, no pre-pass, no e2e/cpu legs")
@@ -387,6 +396,9 @@ def main():
         conw_r = g.precalc()
     torch.cuda.synchronize()
     prepass_s = time.perf_counter() - t0
+    tiles = None
+    if not args.no_autotune and not args.profile and args.form in ("fp64", "fast"):
+        tiles, _ = g.autotune(60)
     n_total = g.n_periods
     B = args.periods_per_step
     fits_per_step = 10 * B
@@ -484,6 +496,8 @@ def main():
         "config": {"workload": WORKLOAD_C5 if args.config == "c5" else WORKLOAD, "form": {"fp64": "fp64 (drop-in, reference operation order)", "fast": "fast fp64 (rearranged, fused; rounding-level differences)", "mixed": "mixed (FP64 model/solve, FP32 derivatives, tcgen05 split-BF16 shape block)"}[args.form], "periods_per_step": B,
                    "fits_per_step": fits_per_step, "l2": "flushed (256 MB write) between timed steps",
                    "prepass": {"fits": None, "seconds": prepass_s, "conw_r": conw_r},
+                   "tiles": {"fch": tiles[0], "rt": tiles[1], "sortseg": tiles[2], "chosen_by": "ps_autotune"}
+                   if tiles else "defaults (32, 32, 1024)",
                    "parallelism": f"period shards x{world}"},
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),

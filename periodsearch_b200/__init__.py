@@ -115,7 +115,7 @@ EXPORTS = (
     "ps_scan_device", "ps_fit", "ps_mrqcof", "ps_model", "ps_info", "ps_get_array", "ps_open_host_only",
     "ps_format_record", "ps_last_error", "ps_kernel_launches", "ps_scan_device_noalloc",
     "ps_batch_open", "ps_batch_scan", "ps_batch_scan_device", "ps_batch_fit_cycles", "ps_batch_close",
-    "ps_fp64_tensor_peak", "ps_chi2_grad", "ps_gn_product",
+    "ps_fp64_tensor_peak", "ps_chi2_grad", "ps_gn_product", "ps_set_tiles", "ps_autotune",
 )
 
 
@@ -155,6 +155,8 @@ def load_library(path: str | None = None):
         "ps_kernel_launches": (ctypes.c_longlong, []),
         "ps_fp64_tensor_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
         "ps_chi2_grad": (ctypes.c_int, [vp, _D, _D, _D]),
+        "ps_set_tiles": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+        "ps_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _D]),
         "ps_gn_product": (ctypes.c_int, [vp, _D, _D, _D]),
     }
     for name, (res, args) in sig.items():
@@ -256,6 +258,19 @@ class PeriodSearch:
         _check(self._lib.ps_model(self._h, _dptr(a), _dptr(y), _dptr(J)))
         return y, J
 
+    def set_tiles(self, fch: int, rt: int, sortseg: int):
+        """Tile shapes (results unchanged): facets per staged chunk and alpha
+        rows per tile of the fast form, points sorted together."""
+        _check(self._lib.ps_set_tiles(self._h, fch, rt, sortseg))
+
+    def autotune(self, n_periods: int = 30):
+        """Time candidate tile shapes on periods 1..n_periods, keep the
+        fastest; returns ((fch, rt, sortseg), seconds)."""
+        t = (ctypes.c_int * 3)()
+        sec = ctypes.c_double()
+        _check(self._lib.ps_autotune(self._h, n_periods, t, ctypes.byref(sec)))
+        return (t[0], t[1], t[2]), sec.value
+
     def chi2_grad(self, a):
         """Matrix-free (chi2, beta) at a; the chi2 gradient over the free
         parameters is -2 beta."""
@@ -321,6 +336,40 @@ class PeriodSearchBatch:
         c = np.zeros(len(self._ctx), dtype=np.int64)
         _check(self._lib.ps_batch_fit_cycles(self._h, c.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
         return c
+
+    @staticmethod
+    def autotune(contexts, n_from, n_to, n_periods: int = 60):
+        """Tile shapes for a batch: tune one asteroid (the work-weighted median
+        by points x periods) with ps_autotune, then time one batch scan of
+        [n_from, n_to] with those tiles and with the defaults and keep the
+        faster -- one asteroid's optimum need not hold for a whole persistent
+        batch.  Sets the tiles on every context; returns (tiles, seconds)."""
+        import time
+
+        ctxs = list(contexts)
+        nf = np.asarray(n_from)
+        nt = np.asarray(n_to)
+        work = np.array([c.n_points for c in ctxs], dtype=np.float64) * (nt - nf + 1)
+        order = np.argsort(work)
+        k = int(order[np.searchsorted(np.cumsum(work[order]), 0.5 * work.sum())])
+        tuned, _ = ctxs[k].autotune(n_periods)
+        best, tbest = None, None
+        for tiles in dict.fromkeys([(32, 32, 1024), tuple(tuned)]):
+            for c in ctxs:
+                c.set_tiles(*tiles)
+            b = PeriodSearchBatch(ctxs)
+            try:
+                b.scan(nf, nt)  # graph capture and warm-up
+                t0 = time.perf_counter()
+                b.scan(nf, nt)
+                dt = time.perf_counter() - t0
+            finally:
+                b.close()
+            if tbest is None or dt < tbest:
+                best, tbest = tiles, dt
+        for c in ctxs:
+            c.set_tiles(*best)
+        return best, tbest
 
     def close(self):
         if self._h:

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -243,6 +244,9 @@ int upload_static(ps_ctx* c) {
     d.cpl = c->d_cpl.p;
     d.cfc = c->d_cfc.p;
     d.cfs = c->d_cfs.p;
+    d.fch = 32;
+    d.rt = 32;
+    d.sortseg = 1024;
     d.cg_first = c->d_cgf.p;
     d.pole0 = c->d_pole.p;
     d.phi0 = p.phi0;
@@ -544,6 +548,87 @@ int ps_set_conw_r(ps_ctx* c, double conw_r) {
     PSB_CUDA(cudaSetDevice(c->device));
     c->prob.conw_r = conw_r;
     return upload_rows(c);
+}
+
+int ps_set_tiles(ps_ctx* c, int fch, int rt, int sortseg) {
+    int rc = check_ready(c, false);
+    if (rc) return rc;
+    if (c->form == PS_FORM_MIXED) return fail(PS_ERR_ARG, "the mixed form has fixed tiles");
+    if (fch < 4 || fch > 128 || fch % 4 || rt < 4 || rt > 256 || rt % 4 || sortseg < 32 || sortseg > 4096 ||
+        (sortseg & (sortseg - 1)))
+        return fail(PS_ERR_ARG, "tiles: fch and rt multiples of 4 (4..128, 4..256), sortseg a power of 2 (32..4096)");
+    PSB_CUDA(cudaSetDevice(c->device));
+    psb::DevProblem& d = c->dp;
+    const int old[3] = {d.fch, d.rt, d.sortseg};
+    d.fch = fch;
+    d.rt = rt;
+    d.sortseg = sortseg;
+    int threads = 0;
+    const int bps = c->form == PS_FORM_FAST ? psb::fast_max_blocks_per_sm(d, &threads)
+                                            : psb::fp64_max_blocks_per_sm(d, &threads);
+    if (bps <= 0) {
+        d.fch = old[0];
+        d.rt = old[1];
+        d.sortseg = old[2];
+        return fail(PS_ERR_LIMIT, "these tiles do not fit in shared memory");
+    }
+    c->blocks_per_sm = bps;
+    if (c->rows_ready) {
+        PSB_CUDA(cudaMemcpyAsync(c->d_dp.p, &c->dp, sizeof(psb::DevProblem), cudaMemcpyHostToDevice, c->stream));
+        PSB_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return PS_OK;
+}
+
+int ps_autotune(ps_ctx* c, int n_periods, int* tiles, double* seconds) {
+    int rc = check_ready(c, true);
+    if (rc) return rc;
+    if (c->form != PS_FORM_FP64 && c->form != PS_FORM_FAST) return fail(PS_ERR_ARG, "autotune runs the FP64 forms");
+    // at least two waves of fits at two CTAs per SM, so that tiles which
+    // cost occupancy show it
+    const int waves = (2 * 2 * c->sms + 9) / 10;
+    const int np = std::max(1, std::min(std::max(n_periods, waves), c->prob.n_periods()));
+    PSB_CUDA(cudaSetDevice(c->device));
+    PSB_CUDA(c->d_rec.ensure(np));
+    auto timed = [&](double& t) -> int {
+        PSB_CUDA(cudaStreamSynchronize(c->stream));
+        const auto t0 = std::chrono::steady_clock::now();
+        int r = scan_into(c, 1, np, c->d_rec.p, 0);
+        if (r) return r;
+        PSB_CUDA(cudaStreamSynchronize(c->stream));
+        t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return check_device_error(c);
+    };
+    const int start[3] = {c->dp.fch, c->dp.rt, c->dp.sortseg};
+    double t = 0;
+    rc = timed(t);  // warm-up with the current tiles
+    if (rc) return rc;
+    int best[3] = {start[0], start[1], start[2]};
+    double tbest = 1e300;
+    static const int fchs[] = {16, 32, 64}, rts[] = {16, 32, 64}, segs[] = {256, 1024};
+    for (int fch : fchs)
+        for (int rt : rts)
+            for (int seg : segs) {
+                if (c->form == PS_FORM_FP64 && (fch != start[0] || rt != start[1])) continue;  // only the sort segment
+                if (ps_set_tiles(c, fch, rt, seg) != PS_OK) continue;
+                rc = timed(t);
+                if (rc) return rc;
+                if (t < tbest) {
+                    tbest = t;
+                    best[0] = fch;
+                    best[1] = rt;
+                    best[2] = seg;
+                }
+            }
+    rc = ps_set_tiles(c, best[0], best[1], best[2]);
+    if (rc) return rc;
+    if (tiles) {
+        tiles[0] = best[0];
+        tiles[1] = best[1];
+        tiles[2] = best[2];
+    }
+    if (seconds) *seconds = tbest;
+    return PS_OK;
 }
 
 int ps_n_periods(const ps_ctx* c) { return c ? c->prob.n_periods() : -1; }

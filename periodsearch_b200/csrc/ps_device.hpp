@@ -28,6 +28,9 @@ struct DevProblem {
     const int* free_idx; // [mfit] parameter index of each free parameter
     const double* cg_first;  // [C]
     const double* pole0;     // [10][2]: initial beta' and lambda [rad]
+    // tile shapes (ps_set_tiles / ps_autotune): the fast form's facets per
+    // staged chunk and alpha rows per tile, and the points sorted together
+    int fch, rt, sortseg;
     // mixed-precision form only
     const float* fac32;          // [F][4]: nx, ny, nz, 0 (FP32 copies)
     const uint16_t* bsw;         // [nchunk][2][64 x 64] BF16 hi/lo of Dsph, swizzled K-major tiles

@@ -21,9 +21,11 @@ namespace {
 
 using namespace fitcommon;
 
-constexpr int kFch = 32;     // facets per shared-memory chunk
-constexpr int kRt = 32;      // rows per alpha tile
-constexpr int kSortSeg = 1024;  // points sorted together by viewing direction
+constexpr int kFch = 32;     // facets per shared-memory chunk (reference-order form)
+constexpr int kRt = 32;      // rows per alpha tile (reference-order form)
+// The fast form takes its facet-chunk and alpha row-tile sizes and both forms
+// the point-sort segment from the problem (DevProblem::fch, rt, sortseg):
+// runtime tile shapes, chosen by ps_autotune; no choice changes any result.
 
 // Blocks of the alpha/beta/chi2 accumulation for mfit free parameters: for
 // each even j0 <= mfit - 1, the 4-column blocks k0 = 4 kb of the lower
@@ -64,16 +66,16 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     PSB_TAKE(misc, 32)
     PSB_TAKE(red, 2 * (kThreads / 32) + 2)
     int chunk = kFch * 5 + kFch * P.NCB;
-    if (2 * kFch * (4 + P.NCB) > chunk) chunk = 2 * kFch * (4 + P.NCB);  // fast form: two staged chunks
+    if (2 * P.fch * (4 + P.NCB) > chunk) chunk = 2 * P.fch * (4 + P.NCB);  // fast form: two staged chunks
     const int kB = (P.mfit + 1) & ~1;
     int tile = kRt * (kB + 2) + kRt * (kB + 4);  // alpha tiles Ws, Js
     const int st8 = (kB + 2 + 7) / 8 * 8 + 4;     // fast form: 8-column tiles, two buffers
-    if (2 * kRt * (st8 + 1) > tile) tile = 2 * kRt * (st8 + 1);
+    if (2 * P.rt * (st8 + 1) > tile) tile = 2 * P.rt * (st8 + 1);
     int w = chunk > tile ? chunk : tile;
     if (P.mfit + 2 > w) w = P.mfit + 2;
-    if (kSortSeg > w) w = kSortSeg;  // sort keys (uint64) before the point loop
+    if (P.sortseg > w) w = P.sortseg;  // sort keys (uint64) before the point loop
     if (gj_buf_doubles(P.mfit) > w) w = gj_buf_doubles(P.mfit);  // Gauss-Jordan buffers
-    PSB_TAKE(perm, kSortSeg / 2)
+    PSB_TAKE(perm, P.sortseg / 2)
     PSB_TAKE(work, w)
 #undef PSB_TAKE
     L.ipiv = o;
@@ -188,20 +190,21 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-// Stage facets [f0, f0 + kFch) of the facet table (nx, ny, nz, Darea) and of
+// Stage facets [f0, f0 + fch) of the facet table (nx, ny, nz, Darea) and of
 // dsph into one chunk buffer: asynchronous 16-byte copies, zeros past F.
 template <int NCB>
 __device__ __forceinline__ void stage_chunk_async(const DevProblem& P, int f0, double* fb, double* db) {
-    const int nf = min(kFch, P.F - f0);
+    const int fch = P.fch;
+    const int nf = min(fch, P.F - f0);
     const double* fs = P.fac + (size_t)f0 * 4;
     const double* ds = P.dsph + (size_t)f0 * NCB;
-    for (int i = threadIdx.x; i < kFch * 2; i += kThreads) {
+    for (int i = threadIdx.x; i < fch * 2; i += kThreads) {
         if (i < nf * 2)
             cp_async16(fb + 2 * i, fs + 2 * i);
         else
             reinterpret_cast<double2*>(fb)[i] = make_double2(0.0, 0.0);
     }
-    for (int i = threadIdx.x; i < kFch * (NCB / 2); i += kThreads) {
+    for (int i = threadIdx.x; i < fch * (NCB / 2); i += kThreads) {
         if (i < nf * (NCB / 2))
             cp_async16(db + 2 * i, ds + 2 * i);
         else
@@ -233,18 +236,19 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, q = lane & 3;
     const int F = P.F, C = P.C, npad = P.npad;
-    double* fbuf[2] = {work, work + kFch * (4 + NCB)};
-    double* dbuf[2] = {work + kFch * 4, work + kFch * (4 + NCB) + kFch * 4};
+    const int fch = P.fch, sseg = P.sortseg;
+    double* fbuf[2] = {work, work + fch * (4 + NCB)};
+    double* dbuf[2] = {work + fch * 4, work + fch * (4 + NCB) + fch * 4};
     int* perm = (int*)(sm + L.perm);
     const double cl = misc[M_CL], cls = misc[M_CLS];
     const unsigned full = 0xffffffffu;
-    const int nch = (F + kFch - 1) / kFch;
+    const int nch = (F + fch - 1) / fch;
     constexpr int kSumJobs = (4 + 3 * NCB + kThreads - 1) / kThreads;
     double fsum[kSumJobs];
 #pragma unroll
     for (int u = 0; u < kSumJobs; u++) fsum[u] = 0;
-    for (int s0 = 0; s0 < P.n_points; s0 += kSortSeg) {
-        const int seg = min(kSortSeg, P.n_points - s0);
+    for (int s0 = 0; s0 < P.n_points; s0 += sseg) {
+        const int seg = min(sseg, P.n_points - s0);
         __syncthreads();
         sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
         for (int base = 0; base < seg; base += kPts) {
@@ -283,11 +287,11 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
             cp_async_wait_all();
             __syncthreads();
             for (int ch = 0; ch < nch; ch++) {
-                const int f0 = ch * kFch;
-                if (ch + 1 < nch) stage_chunk_async<NCB>(P, f0 + kFch, fbuf[(ch + 1) & 1], dbuf[(ch + 1) & 1]);
+                const int f0 = ch * fch;
+                if (ch + 1 < nch) stage_chunk_async<NCB>(P, f0 + fch, fbuf[(ch + 1) & 1], dbuf[(ch + 1) & 1]);
                 const double* fb = fbuf[ch & 1];
                 const double* db = dbuf[ch & 1];
-                const int nf = min(kFch, F - f0);
+                const int nf = min(fch, F - f0);
                 if (s0 == 0 && base == 0) {
                     // the facet sums (convexity residuals and derivatives, facet-area
                     // sum) from the staged chunk, facets in order, one thread per sum
@@ -433,8 +437,9 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
     const int kB = (mfit + 1) & ~1;
     const int T = (kB + 2 + 7) / 8, st = T * 8 + 4, ktB = kB / 8;
     const int ntri = T * (T + 1) / 2, ntile = ntri + ktB;
-    double* Js[2] = {work, work + kRt * (st + 1)};
-    double* wv[2] = {work + kRt * st, work + kRt * (st + 1) + kRt * st};
+    const int rt = P.rt;
+    double* Js[2] = {work, work + rt * (st + 1)};
+    double* wv[2] = {work + rt * st, work + rt * (st + 1) + rt * st};
     int tj[kTiles], tk[kTiles];
     double acc[kTiles][2];
 #pragma unroll
@@ -453,7 +458,7 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
         acc[i][0] = acc[i][1] = 0;
     }
     auto issue = [&](int r0, int b) {
-        const int nr = min(kRt, nrows - r0);
+        const int nr = min(rt, nrows - r0);
         for (int idx = tid; idx < nr * mfit; idx += kThreads) {
             const int j = idx / nr, r = idx - j * nr;
             cp_async8(Js[b] + r * st + j, Jt + (size_t)P.free_idx[j] * npad + r0 + r);
@@ -461,11 +466,11 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
         cp_async_commit();
     };
     __syncthreads();
-    for (int i = tid; i < 2 * kRt * (st + 1); i += kThreads) work[i] = 0.0;
+    for (int i = tid; i < 2 * rt * (st + 1); i += kThreads) work[i] = 0.0;
     __syncthreads();
-    const int ntl = (nrows + kRt - 1) / kRt;
+    const int ntl = (nrows + rt - 1) / rt;
     issue(0, 0);
-    if (tid < kRt) {
+    if (tid < rt) {
         const double dy = tid < nrows ? P.yobs[tid] - yt[tid] : 0.0;
         Js[0][tid * st + kB] = dy;
         wv[0][tid] = tid < nrows ? P.sig2i[tid] * P.wght[tid] : 0.0;
@@ -473,13 +478,13 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
     cp_async_wait_all();
     __syncthreads();
     for (int t = 0; t < ntl; t++) {
-        const int b = t & 1, r0 = t * kRt;
-        const int nr4 = (min(kRt, nrows - r0) + 3) & ~3;
+        const int b = t & 1, r0 = t * rt;
+        const int nr4 = (min(rt, nrows - r0) + 3) & ~3;
         double ndy = 0.0, nw = 0.0;
         if (t + 1 < ntl) {
-            const int r1 = r0 + kRt;
+            const int r1 = r0 + rt;
             issue(r1, b ^ 1);
-            if (tid < kRt && r1 + tid < nrows) {
+            if (tid < rt && r1 + tid < nrows) {
                 ndy = P.yobs[r1 + tid] - yt[r1 + tid];
                 nw = P.sig2i[r1 + tid] * P.wght[r1 + tid];
             }
@@ -493,7 +498,7 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
             for (int i = 0; i < kTiles; i++)
                 if (tj[i] >= 0) dmma_8x8x4(acc[i][0], acc[i][1], row[tj[i]] * w, row[tk[i]]);
         }
-        if (t + 1 < ntl && tid < kRt) {
+        if (t + 1 < ntl && tid < rt) {
             Js[b ^ 1][tid * st + kB] = ndy;
             wv[b ^ 1][tid] = nw;  // zero past the last row
         }
@@ -611,8 +616,8 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
         double* s_dg = work + kFch * 5;
         int* perm = (int*)(sm + L.perm);
         const double cl = misc[M_CL], cls = misc[M_CLS];
-        for (int s0 = 0; s0 < P.n_points; s0 += kSortSeg) {
-        const int seg = min(kSortSeg, P.n_points - s0);
+        for (int s0 = 0; s0 < P.n_points; s0 += P.sortseg) {
+        const int seg = min(P.sortseg, P.n_points - s0);
         __syncthreads();
         sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
         for (int base = 0; base < seg; base += kThreads) {
