@@ -14,7 +14,7 @@ Two rules:
   unit of the last printed digit, periods within 1e-9 relative or half a
   printed digit, the dark-facet column within 1e-6 or half a printed digit,
   and the same order of the K best periods by chi2 (K = 1, 10, 20); the pole
-  angles are reported, not judged.  With the unrounded side files
+  angles are reported, not checked.  With the unrounded side files
   (``.full``, the same six columns at full precision) the printed-digit
   floors drop out.
 
@@ -89,7 +89,7 @@ def strict_report(a: np.ndarray, b: np.ndarray, tol: float = 1e-9, printed: bool
         x, y = a[key], b[key]
         d = np.abs(x - y)
         if key in ("lambda_deg", "beta_deg"):
-            rep["worst"][key] = float(np.max(d))  # reported, not judged: flat chi2 valleys move them
+            rep["worst"][key] = float(np.max(d))  # reported, not checked: flat chi2 valleys move them
             continue
         floor = 0.5 * PRINT_STEP[i] * (1 + 1e-9) if printed else 0.0
         if key in rel:
