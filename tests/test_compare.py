@@ -57,3 +57,16 @@ def test_parse_errors(tmp_path):
     assert compare.main([str(bad), good, "--rule", "boinc"]) == 2
     bad.write_text("12.0  0.1\n")
     assert compare.main([str(bad), good]) == 2
+
+
+def test_reference_validator_known_answer(tmp_path):
+    """The reference's TestValidator case (period_search_pure_cpu_win/
+    UnitTest_pure_cpu_win/InnerFunctionsTests.cpp:1059-1095): the AVX and the
+    plain CPU builds' records for one period match under the validator rule;
+    the strict rule (1e-9 or half a printed digit) tells them apart."""
+    a = tmp_path / "avx"
+    b = tmp_path / "cpu"
+    a.write_text("17.20899774  0.167425  3.307656  1.6   96   59\n")
+    b.write_text("17.20899838  0.167423  3.307587  1.6   96   59\n")
+    assert compare.main([str(a), str(b), "--rule", "boinc"]) == 0
+    assert compare.main([str(a), str(b), "--rule", "strict"]) == 1
