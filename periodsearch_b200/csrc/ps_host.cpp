@@ -6,6 +6,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 namespace psb {
 namespace {
@@ -477,6 +480,41 @@ int finish_from_arrays(Problem& p, std::string& err) {
     return 0;
 }
 
+// The facet grid and its spherical-harmonic tables (trifac, areanorm,
+// sphfunc) depend only on (nrows, lmax, mmax): computed once per process and
+// copied for every further asteroid on the same grid.
+void grid_tables(Problem& p) {
+    struct Tables {
+        std::vector<int> ifp;
+        std::vector<double> nor, darea, at, af, pleg, dsph, fc, fs;
+    };
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int>, Tables> cache;
+    const auto key = std::make_tuple(p.nrows, p.lmax, p.mmax);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) {
+            const Tables& t = it->second;
+            p.ifp = t.ifp;
+            p.nor = t.nor;
+            p.darea = t.darea;
+            p.at = t.at;
+            p.af = t.af;
+            p.pleg = t.pleg;
+            p.dsph = t.dsph;
+            p.fc = t.fc;
+            p.fs = t.fs;
+            return;
+        }
+    }
+    trifac(p.nrows, p.ifp);
+    areanorm(p);
+    sphfunc(p);
+    std::lock_guard<std::mutex> lock(mu);
+    if (cache.size() < 16) cache.emplace(key, Tables{p.ifp, p.nor, p.darea, p.at, p.af, p.pleg, p.dsph, p.fc, p.fs});
+}
+
 int setup_geometry(Problem& p, std::string& err) {
     p.ncoef = 0;
     for (int m = 0; m <= p.mmax; m++)
@@ -488,9 +526,7 @@ int setup_geometry(Problem& p, std::string& err) {
     p.ndir = 4 * p.nrows * p.nrows + 2;
     p.nphpar = 3;
     p.ma = p.ncoef + 5 + p.nphpar;
-    trifac(p.nrows, p.ifp);
-    areanorm(p);
-    sphfunc(p);
+    grid_tables(p);
     if (ellfit(p) != 0) {
         err = "singular matrix in the ellipsoid fit (ludcmp)";
         return 4;
