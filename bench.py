@@ -488,6 +488,15 @@ def main():
                            "mixed": "mixed_fit_kernel (FP64/FP32 SIMT + tcgen05 split-BF16 shape block)"}[args.form],
                 "flop_per_launch": flop_launch,
                 "flop_rule": "per evaluation 2 N F C + N mfit (mfit + 1), 51 evaluations per fit"}
+    # DRAM bytes per fit from ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+    # on the 300-fit profile launch of the c2 workload (bench.py --profile),
+    # scaled to this launch's fits: the per-CTA J scratch (356 KB) stays in L2
+    # at one fit per SM and is evicted at two
+    per_fit = {"fast": 5.51e7, "fp64": 5.20e6}.get(args.form) if args.config == "c2" else None
+    if per_fit:
+        roofline["traffic"] = per_fit * fits_per_step
+        roofline["traffic_source"] = ("ncu dram bytes of the 300-fit c2 profile launch of this form, "
+                                      "scaled by fits per launch")
     line = {
         "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * t_max / args.steps, "higher_is_better": True,
