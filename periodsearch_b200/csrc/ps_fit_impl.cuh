@@ -66,7 +66,8 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     PSB_TAKE(misc, 32)
     PSB_TAKE(red, 2 * (kThreads / 32) + 2)
     int chunk = kFch * 5 + kFch * P.NCB;
-    if (2 * P.fch * (4 + P.NCB) > chunk) chunk = 2 * P.fch * (4 + P.NCB);  // fast form: two staged chunks
+    // fast form: two staged chunks, dsph rows padded to NCB + 4 doubles
+    if (2 * P.fch * (8 + P.NCB) > chunk) chunk = 2 * P.fch * (8 + P.NCB);
     const int kB = (P.mfit + 1) & ~1;
     int tile = kRt * (kB + 2) + kRt * (kB + 4);  // alpha tiles Ws, Js
     const int st8 = (kB + 2 + 7) / 8 * 8 + 4;     // fast form: 8-column tiles, two buffers
@@ -192,6 +193,13 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 // Stage facets [f0, f0 + fch) of the facet table (nx, ny, nz, Darea) and of
 // dsph into one chunk buffer: asynchronous 16-byte copies, zeros past F.
+// Row stride (doubles) of a staged dsph chunk.  The m8n8k4 B fragment has
+// lane (g, q) read row q, column g + 8t: with a stride of 4 or 12 mod 16
+// doubles the 16 lanes of each half-warp fall on distinct bank pairs (an
+// unpadded stride of NCB = 0 or 8 mod 16 puts two lanes on each pair).
+template <int NCB>
+constexpr int kDs = NCB + 4;
+
 template <int NCB>
 __device__ __forceinline__ void stage_chunk_async(const DevProblem& P, int f0, double* fb, double* db) {
     const int fch = P.fch;
@@ -205,10 +213,11 @@ __device__ __forceinline__ void stage_chunk_async(const DevProblem& P, int f0, d
             reinterpret_cast<double2*>(fb)[i] = make_double2(0.0, 0.0);
     }
     for (int i = threadIdx.x; i < fch * (NCB / 2); i += kThreads) {
+        const int ff = i / (NCB / 2), c = 2 * (i - ff * (NCB / 2));
         if (i < nf * (NCB / 2))
-            cp_async16(db + 2 * i, ds + 2 * i);
+            cp_async16(db + ff * kDs<NCB> + c, ds + 2 * i);
         else
-            reinterpret_cast<double2*>(db)[i] = make_double2(0.0, 0.0);
+            *reinterpret_cast<double2*>(db + ff * kDs<NCB> + c) = make_double2(0.0, 0.0);
     }
     cp_async_commit();
 }
@@ -225,20 +234,25 @@ __device__ __forceinline__ void stage_chunk_async(const DevProblem& P, int f0, d
 // skips its MMAs.  Facet chunks are staged with asynchronous copies, one chunk
 // ahead.  Sums split by facet (lane q takes facets q mod 4) are combined at
 // the end: the form differs from the reference order by rounding only.
-template <int NCB>
+// kX1 (C = NCB - 7, i.e. C = 1 mod 8 as for every even lmax = mmax): the last
+// 8-column tile would carry a single coefficient, so coefficient C - 1 is
+// summed per lane on the FP64 pipe (one FMA per visible pair) and the MMA
+// sequence covers the first NCB - 8 columns.
+template <int NCB, bool kX1>
 __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm, const Layout& L, const double* B,
                                                 const double* D, double* misc, const double* g_f,
                                                 const double* area, double* dres, double* work, double* Jt,
                                                 double* yt) {
-    constexpr int NT = NCB / 8;                  // accumulator tiles per 8 points
+    constexpr int NT = kX1 ? NCB / 8 - 1 : NCB / 8;  // MMA accumulator tiles per 8 points
+    static_assert(NT > 0, "kX1 needs NCB >= 16");
     constexpr int kMT = 1;                       // point tiles per warp
     constexpr int kPts = (kThreads / 32) * 8 * kMT;  // points per pass
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, q = lane & 3;
     const int F = P.F, C = P.C, npad = P.npad;
     const int fch = P.fch, sseg = P.sortseg;
-    double* fbuf[2] = {work, work + fch * (4 + NCB)};
-    double* dbuf[2] = {work + fch * 4, work + fch * (4 + NCB) + fch * 4};
+    double* fbuf[2] = {work, work + fch * (4 + kDs<NCB>)};
+    double* dbuf[2] = {work + fch * 4, work + fch * (4 + kDs<NCB>) + fch * 4};
     int* perm = (int*)(sm + L.perm);
     const double cl = misc[M_CL], cls = misc[M_CLS];
     const unsigned full = 0xffffffffu;
@@ -273,12 +287,12 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
                 }
             }
             double acc[kMT][NT][2];
-            double br[kMT], T[kMT][3], S[kMT][3], s_cl[kMT], s_cls[kMT];
+            double br[kMT], T[kMT][3], S[kMT][3], s_cl[kMT], s_cls[kMT], x1[kMT];
 #pragma unroll
             for (int i = 0; i < kMT; i++) {
 #pragma unroll
                 for (int t = 0; t < NT; t++) acc[i][t][0] = acc[i][t][1] = 0;
-                br[i] = s_cl[i] = s_cls[i] = 0;
+                br[i] = s_cl[i] = s_cls[i] = x1[i] = 0;
 #pragma unroll
                 for (int c = 0; c < 3; c++) T[i][c] = S[i][c] = 0;
             }
@@ -306,7 +320,7 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
                         } else {
                             const int nc = (job - 4) / C, jj = (job - 4) - nc * C;
                             for (int ff = 0; ff < nf; ff++) {
-                                const double dg = g_f[f0 + ff] * db[ff * NCB + jj];
+                                const double dg = g_f[f0 + ff] * db[ff * kDs<NCB> + jj];
                                 sacc += fb[ff * 4 + 3] * dg * fb[ff * 4 + nc];
                             }
                         }
@@ -344,13 +358,14 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
                             const double mm = mu * mu0 * ar;
                             s_cl[i] += mm;
                             s_cls[i] = fma(mm, r, s_cls[i]);
+                            if (kX1) x1[i] = fma(av[i], db[ff * kDs<NCB> + 8 * NT], x1[i]);
                         }
                     }
                     bool some = false;
 #pragma unroll
                     for (int i = 0; i < kMT; i++) some = some || any[i];
                     if (!some) continue;
-                    const double* brow = db + ff * NCB + g;
+                    const double* brow = db + ff * kDs<NCB> + g;
 #pragma unroll
                     for (int t = 0; t < NT; t++) {
                         const double bv = brow[t * 8];
@@ -370,6 +385,7 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
                     br[i] += __shfl_xor_sync(full, br[i], o);
                     s_cl[i] += __shfl_xor_sync(full, s_cl[i], o);
                     s_cls[i] += __shfl_xor_sync(full, s_cls[i], o);
+                    if (kX1) x1[i] += __shfl_xor_sync(full, x1[i], o);
 #pragma unroll
                     for (int c = 0; c < 3; c++) {
                         T[i][c] += __shfl_xor_sync(full, T[i][c], o);
@@ -387,6 +403,7 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
                         const int k = t * 8 + 2 * q + jj;
                         if (k < C) Jt[(size_t)k * npad + p[i]] = sc * acc[i][t][jj];
                     }
+                if (kX1 && q == 0) Jt[(size_t)(8 * NT) * npad + p[i]] = sc * x1[i];
                 if (q == 0) {
 #pragma unroll
                     for (int k = 0; k < 3; k++) {
@@ -608,7 +625,14 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
         }
     }
     if constexpr (kFast) {
-        point_loop_fast<NCB>(P, sm, L, B, D, misc, g, area, dres, work, Jt, yt);
+        if constexpr (NCB >= 16) {
+            if (C == NCB - 7)
+                point_loop_fast<NCB, true>(P, sm, L, B, D, misc, g, area, dres, work, Jt, yt);
+            else
+                point_loop_fast<NCB, false>(P, sm, L, B, D, misc, g, area, dres, work, Jt, yt);
+        } else {
+            point_loop_fast<NCB, false>(P, sm, L, B, D, misc, g, area, dres, work, Jt, yt);
+        }
     } else {
         // bright.c:54-125 for every data point, in segments of points sorted by
         // viewing direction
