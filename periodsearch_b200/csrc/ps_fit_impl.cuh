@@ -48,7 +48,7 @@ struct Layout {
 
 __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     Layout L;
-    int o = 0;
+    int o = 2;  // doubles 0-1: the fit kernel's work-queue slots (fit index, asteroid)
 #define PSB_TAKE(field, n) \
     L.field = o;           \
     o += ((n) + 1) & ~1;
@@ -251,8 +251,11 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
     const int g = lane >> 2, q = lane & 3;
     const int F = P.F, C = P.C, npad = P.npad;
     const int fch = P.fch, sseg = P.sortseg;
-    double* fbuf[2] = {work, work + fch * (4 + kDs<NCB>)};
-    double* dbuf[2] = {work + fch * 4, work + fch * (4 + kDs<NCB>) + fch * 4};
+    // chunk buffer b at work + b * cstride: fch facet rows, then fch dsph rows.
+    // Buffers are selected by arithmetic on `work`, not from an array of
+    // pointers: a dynamically indexed pointer array would live in local memory
+    // and every load through its elements become a generic load.
+    const int cstride = fch * (4 + kDs<NCB>);
     int* perm = (int*)(sm + L.perm);
     const double cl = misc[M_CL], cls = misc[M_CLS];
     const unsigned full = 0xffffffffu;
@@ -297,14 +300,15 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
                 for (int c = 0; c < 3; c++) T[i][c] = S[i][c] = 0;
             }
             __syncthreads();
-            stage_chunk_async<NCB>(P, 0, fbuf[0], dbuf[0]);
+            stage_chunk_async<NCB>(P, 0, work, work + fch * 4);
             cp_async_wait_all();
             __syncthreads();
             for (int ch = 0; ch < nch; ch++) {
                 const int f0 = ch * fch;
-                if (ch + 1 < nch) stage_chunk_async<NCB>(P, f0 + fch, fbuf[(ch + 1) & 1], dbuf[(ch + 1) & 1]);
-                const double* fb = fbuf[ch & 1];
-                const double* db = dbuf[ch & 1];
+                double* nb = work + ((ch + 1) & 1) * cstride;
+                if (ch + 1 < nch) stage_chunk_async<NCB>(P, f0 + fch, nb, nb + fch * 4);
+                const double* fb = work + (ch & 1) * cstride;
+                const double* db = fb + fch * 4;
                 const int nf = min(fch, F - f0);
                 if (s0 == 0 && base == 0) {
                     // the facet sums (convexity residuals and derivatives, facet-area
@@ -455,8 +459,9 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
     const int T = (kB + 2 + 7) / 8, st = T * 8 + 4, ktB = kB / 8;
     const int ntri = T * (T + 1) / 2, ntile = ntri + ktB;
     const int rt = P.rt;
-    double* Js[2] = {work, work + rt * (st + 1)};
-    double* wv[2] = {work + rt * st, work + rt * (st + 1) + rt * st};
+    // buffer b: Js at work + b * bstride (rt rows of st), then the rt weights
+    // (arithmetic on `work`, not a pointer array: see point_loop_fast)
+    const int bstride = rt * (st + 1);
     int tj[kTiles], tk[kTiles];
     double acc[kTiles][2];
 #pragma unroll
@@ -478,7 +483,7 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
         const int nr = min(rt, nrows - r0);
         for (int idx = tid; idx < nr * mfit; idx += kThreads) {
             const int j = idx / nr, r = idx - j * nr;
-            cp_async8(Js[b] + r * st + j, Jt + (size_t)P.free_idx[j] * npad + r0 + r);
+            cp_async8(work + b * bstride + r * st + j, Jt + (size_t)P.free_idx[j] * npad + r0 + r);
         }
         cp_async_commit();
     };
@@ -489,8 +494,8 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
     issue(0, 0);
     if (tid < rt) {
         const double dy = tid < nrows ? P.yobs[tid] - yt[tid] : 0.0;
-        Js[0][tid * st + kB] = dy;
-        wv[0][tid] = tid < nrows ? P.sig2i[tid] * P.wght[tid] : 0.0;
+        work[tid * st + kB] = dy;
+        work[rt * st + tid] = tid < nrows ? P.sig2i[tid] * P.wght[tid] : 0.0;
     }
     cp_async_wait_all();
     __syncthreads();
@@ -506,8 +511,8 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
                 nw = P.sig2i[r1 + tid] * P.wght[r1 + tid];
             }
         }
-        const double* jb = Js[b];
-        const double* wb = wv[b];
+        const double* jb = work + b * bstride;
+        const double* wb = jb + rt * st;
         for (int rr = 0; rr < nr4; rr += 4) {
             const double* row = jb + (rr + q) * st + g;
             const double w = wb[rr + q];
@@ -516,8 +521,9 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
                 if (tj[i] >= 0) dmma_8x8x4(acc[i][0], acc[i][1], row[tj[i]] * w, row[tk[i]]);
         }
         if (t + 1 < ntl && tid < rt) {
-            Js[b ^ 1][tid * st + kB] = ndy;
-            wv[b ^ 1][tid] = nw;  // zero past the last row
+            double* jn = work + (b ^ 1) * bstride;
+            jn[tid * st + kB] = ndy;
+            jn[rt * st + tid] = nw;  // zero past the last row
         }
         cp_async_wait_all();
         __syncthreads();
@@ -544,14 +550,22 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
 }
 
 // One model evaluation, the reference's mrqcof (mrqcof.c:16-148) at
-// parameters a (shared memory).  Writes the symmetrised alpha and beta into
-// alpha_out / beta_out (shared memory) and chi2, the convexity residuals
-// (= the driver's chck, period_search_BOINC.cpp:876-880) and the facet-area
-// sum into misc.  J^T (ma columns of npad rows) and y go to the CTA's
-// scratch.  All threads enter and leave together.
+// parameters a (shared memory, at offset a_off).  Writes the symmetrised
+// alpha and beta into alpha_out / beta_out (shared memory, offsets alpha_off
+// and beta_off) and chi2, the convexity residuals (= the driver's chck,
+// period_search_BOINC.cpp:876-880) and the facet-area sum into misc.  J^T (ma
+// columns of npad rows) and y go to the CTA's scratch.  All threads enter and
+// leave together.  The shared-memory operands are passed as offsets from the
+// dynamic shared-memory base declared here, not as pointers: a pointer
+// argument of this out-of-line function would be a generic address, and every
+// access through it a generic load or store instead of a shared-memory one.
 template <int NCB, bool kFast>
-__device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double* sm, const double* a,
-                                      double* alpha_out, double* beta_out, double* Jt, double* yt) {
+__device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_off, int alpha_off, int beta_off,
+                                      double* Jt, double* yt) {
+    extern __shared__ __align__(16) double sm[];
+    const double* a = sm + a_off;
+    double* alpha_out = sm + alpha_off;
+    double* beta_out = sm + beta_off;
     const DevProblem& P = *Pp;
     const Layout L = make_layout(P);
     const int tid = threadIdx.x;
@@ -896,8 +910,13 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, double*
 
 template <int NCB, bool kFast>
 __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_kernel(const DevProblem* __restrict__ Parr, FitBatch Bt) {
+    // No static __shared__ variable may be declared in these kernels: with
+    // one, the dynamic region would start after it here but not in the
+    // out-of-line evaluate(), which addresses it through its own extern
+    // declaration.  The queue slots live in the first 16 bytes instead.
     extern __shared__ __align__(16) double sm[];
-    __shared__ int s_work, s_ast;
+    int& s_work = reinterpret_cast<int*>(sm)[0];
+    int& s_ast = reinterpret_cast<int*>(sm)[1];
     const int tid = threadIdx.x;
     int cur_mfit = -1, cur_ent = -1;
     for (;;) {
@@ -997,7 +1016,7 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
         while (((niter < P.n_iter_max) && (iter_diff > P.iter_diff_max)) || (niter < P.n_iter_min)) {
             if (alamda < 0) {
                 alamda = P.alamda_start;
-                evaluate<NCB, kFast>(Pp, sm, cg, alpha, beta, Jt, yt);
+                evaluate<NCB, kFast>(Pp, (int)(cg - sm), (int)(alpha - sm), (int)(beta - sm), Jt, yt);
                 ochisq = misc[M_CHISQ];
                 cur0 = misc[M_CHK0];
                 cur1 = misc[M_CHK0 + 1];
@@ -1019,7 +1038,9 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
                     atry[l] = cg[l] + da[j];
                 }
                 __syncthreads();
-                evaluate<NCB, kFast>(Pp, sm, atry, covar, da, Jt, yt);
+                // alpha/covar and beta/da trade places on every accepted step: the
+                // offsets follow the pointers
+                evaluate<NCB, kFast>(Pp, (int)(atry - sm), (int)(covar - sm), (int)(da - sm), Jt, yt);
                 const double temp = misc[M_CHISQ];
                 chisq = temp;
                 s_last = misc[M_SAREA];
@@ -1093,7 +1114,7 @@ __global__ void __launch_bounds__(kThreads, 1) eval_kernel(const DevProblem* __r
     alpha_jobs(P.mfit, (int*)(sm + L.ent));
     for (int i = tid; i < P.ma; i += kThreads) cg[i] = E.a[i];
     __syncthreads();
-    evaluate<NCB, kFast>(Pp, sm, cg, sm + L.alpha, sm + L.beta, Jt, yt);
+    evaluate<NCB, kFast>(Pp, L.cg, L.alpha, L.beta, Jt, yt);
     for (int i = tid; i < P.mfit * P.mfit; i += kThreads) E.alpha[i] = sm[L.alpha + i];
     for (int i = tid; i < P.mfit; i += kThreads) E.beta[i] = sm[L.beta + i];
     if (tid == 0) E.chisq[0] = sm[L.misc + M_CHISQ];
