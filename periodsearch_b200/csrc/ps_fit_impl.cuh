@@ -59,7 +59,7 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     PSB_TAKE(beta, P.mfit)
     PSB_TAKE(da, P.mfit)
     PSB_TAKE(g, P.F)
-    PSB_TAKE(area, P.F)
+    PSB_TAKE(area, P.F + 128)  // zeros past F: the fast point loop reads whole chunks
     PSB_TAKE(dres, 3 * P.C)
     PSB_TAKE(dave, P.ma + 2)
     PSB_TAKE(blm, 28)
@@ -331,18 +331,19 @@ __device__ __forceinline__ void point_loop_fast(const DevProblem& P, double* sm,
                         fsum[u] = sacc;
                     }
                 }
+                // Facets past F (zero rows in the staged chunk, zero area) and
+                // inactive lanes (e = e0 = 0) have mu = mu0 = 0: not visible.
                 for (int j = 0; j < nf; j += 4) {
                     const int ff = j + q;
-                    const bool valid = f0 + ff < F;
                     const double nx = fb[ff * 4 + 0], ny = fb[ff * 4 + 1], nz = fb[ff * 4 + 2];
-                    const double ar = valid ? area[f0 + ff] : 0.0;
+                    const double ar = area[f0 + ff];
                     double av[kMT];
                     bool any[kMT];
 #pragma unroll
                     for (int i = 0; i < kMT; i++) {
                         const double mu = e[i][0] * nx + e[i][1] * ny + e[i][2] * nz;
                         const double mu0 = e0[i][0] * nx + e0[i][1] * ny + e0[i][2] * nz;
-                        const bool vis = act[i] && valid && (mu > kTinyD) && (mu0 > kTinyD);
+                        const bool vis = (mu > kTinyD) && (mu0 > kTinyD);
                         any[i] = __any_sync(full, vis);
                         av[i] = 0;
                         if (vis) {
@@ -612,6 +613,7 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_o
         g[f] = gi;
         area[f] = P.fac[(size_t)f * 4 + 3] * gi;
     }
+    for (int f = F + tid; f < F + 128; f += kThreads) area[f] = 0.0;
     __syncthreads();
     // Sequential facet sums: chck / conv residuals (conv.c:22-27), the
     // facet-area sum (period_search_BOINC.cpp:900-902) and the conv-row shape
