@@ -116,6 +116,35 @@ def _oracle_worker(args):
     return len(fits)
 
 
+def _oracle_eval_worker(args):
+    path, conw_r, n, pole = args
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pso
+
+    o = pso.Oracle(path)
+    o.set_conw_r(conw_r)
+    a = o.initial_parameters(o.freq(n), pole)
+    t0 = time.perf_counter()
+    o.mrqcof(a)
+    return time.perf_counter() - t0
+
+
+def cpu_eval_sample(path, conw_r, n_first, evals_per_fit):
+    """For workloads whose fits take minutes on a CPU core: time one model
+    evaluation (mrqcof: model, Jacobian, alpha, beta) of the CPU oracle per
+    host core and convert with the evaluations of one fit (the LM solve is
+    negligible beside them on a CPU).  Returns (fits/s, cores, evals, s)."""
+    import multiprocessing as mp
+
+    cores = os.cpu_count() or 1
+    jobs = [(path, conw_r, n_first + c // 10, c % 10 + 1) for c in range(cores)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        ts = pool.map(_oracle_eval_worker, jobs)
+    t_eval = statistics.mean(ts)
+    return cores / (t_eval * evals_per_fit), cores, cores, max(ts)
+
+
 def cpu_sample(path, conw_r, n_first, fits_per_core=2):
     """Time the CPU oracle on cores x fits_per_core fits of the workload,
     one process per host core (the reference is single-threaded)."""
@@ -193,18 +222,47 @@ def ref_cpu_sample(path, n_first, periods_per_proc=1):
     return done / dt, cores, done, dt
 
 
+# The reference application keeps its data in static arrays
+# (constants.h: MAX_N_FAC = 1000 facets, MAX_N_OBS = 20000 points); a
+# workload beyond them (the lmax = 8, 2048-facet, 20 000-point one) cannot run
+# there, and the CPU leg times the restatement instead.
+REF_LIMITS = {"facets": 1000, "points": 20000}
+
+
+def ref_cpu_sample_or_none(path, n_first):
+    """ref_cpu_sample, or (None, reason) when the reference application is
+    not built or the workload exceeds its static array sizes."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import pso
+
+    o = pso.Oracle(path)
+    o.set_conw_r(o.conw_r)  # builds the shape model (facet count)
+    if o.numfac > REF_LIMITS["facets"] or o.n_points > REF_LIMITS["points"]:
+        return None, (f"the reference application holds at most {REF_LIMITS['facets']} facets and "
+                      f"{REF_LIMITS['points']} points (MAX_N_FAC, MAX_N_OBS); this workload has "
+                      f"{o.numfac} facets, {o.n_points} points")
+    r = ref_cpu_sample(path, n_first)
+    return r, None if r is not None else "the reference application is not built"
+
+
 def run_reference(args, path, rank):
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import pso
 
-    conw_r = pso.Oracle(path).conw_r  # the pre-pass value is not needed for timing a fit
-    kind = "reference" if os.path.exists(REF_EXE) else "port"
+    o = pso.Oracle(path)
+    conw_r = o.conw_r  # the pre-pass value is not needed for timing a fit
+    o.set_conw_r(conw_r)  # builds the shape model (facet count)
+    fits_ref = o.numfac <= REF_LIMITS["facets"] and o.n_points <= REF_LIMITS["points"]
+    kind = "reference" if os.path.exists(REF_EXE) and fits_ref else "port"
     vals = []
     for s in range(args.warmup + args.steps):
         if kind == "reference":
             v, cores, done, dt = ref_cpu_sample(path, 1 + 37 * s)
+        elif args.config == "c5":
+            v, cores, done, dt = cpu_eval_sample(path, conw_r, 1 + 37 * s, 51)
+            done, dt = v * dt, dt  # fits-equivalent of the timed evaluations
         else:
             v, cores, done, dt = cpu_sample(path, conw_r, 1 + 37 * s, fits_per_core=1)
         if s >= args.warmup:
@@ -214,11 +272,15 @@ def run_reference(args, path, rank):
         "impl": "reference", "metric": METRIC, "value": value, "unit": "fits/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * statistics.mean(t for _, _, t in vals),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "form": "reference CPU application (oracle/_ref, -O3)" if kind == "reference"
+        "config": {"workload": WORKLOAD_C5 if args.config == "c5" else WORKLOAD,
+                   "form": "reference CPU application (oracle/_ref, -O3)" if kind == "reference"
                    else "cpu oracle (reference restated, bit-exact)"},
         "cpu_baseline": {"value": value, "unit": "fits/s", "cores": cores, "kind": kind,
                          "sample": (f"{cores} processes x 1 trial period (10 fits) per step, pre-pass skipped"
                                     if kind == "reference" else
+                                    f"{cores} processes x 1 model evaluation per step, converted at 51 "
+                                    f"evaluations per fit; the reference application's static arrays hold at most "
+                                    f"{REF_LIMITS['facets']} facets" if args.config == "c5" else
                                     f"{cores} processes x 1 fit per step (consecutive periods x poles)")},
         "e2e": {"value": value, "unit": "fits/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -515,16 +577,22 @@ def main():
         "clocks": clocks,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        r = ref_cpu_sample(path, 1)
+        r, why = ref_cpu_sample_or_none(path, 1)
         if r is not None:
             v, cores, done, dt = r
             line["cpu_baseline"] = {"value": v, "unit": "fits/s", "cores": cores, "kind": "reference",
                                     "sample": f"{done} fits: {cores} processes of the reference CPU application x 1 "
                                               f"trial period, pre-pass skipped, {dt:.1f} s"}
         else:
-            v, cores, done, dt = cpu_sample(path, conw_r, 1)
+            if args.config == "c5":
+                v, cores, done, dt = cpu_eval_sample(path, conw_r, 1, 51)
+                sample = (f"{done} model evaluations (one per process) of the CPU oracle, {dt:.1f} s, "
+                          f"converted at 51 evaluations per 50-iteration fit")
+            else:
+                v, cores, done, dt = cpu_sample(path, conw_r, 1)
+                sample = f"{done} fits ({cores} processes x 2) of the same workload, {dt:.1f} s"
             line["cpu_baseline"] = {"value": v, "unit": "fits/s", "cores": cores, "kind": "port",
-                                    "sample": f"{done} fits ({cores} processes x 2) of the same workload, {dt:.1f} s"}
+                                    "sample": sample + (f"; {why}" if why else "")}
     g.close()
     if dist:
         dist.barrier()
