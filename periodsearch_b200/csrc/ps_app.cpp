@@ -8,8 +8,13 @@
 // reference's 6-column format and checkpoints to DIR/period_search_state
 // after every chunk of trial periods ("nlines newConw conw_r", the CUDA
 // application's 3-field form; a 1-field CPU-style state is also accepted,
-// which re-runs the convexity pre-pass like the CPU application does).  On
-// restart the scan resumes at nlines + 1 and the output is appended.
+// which re-runs the convexity pre-pass like the CPU application does, and
+// the 5-field "nlines newConw conw_r sum_dark_facet ntestperiods" form of the
+// pure-CPU and OpenCL applications
+// (period_search_pure_cpu_win/period_search/period_search_BOINC.cpp:91,257)
+// is read by its first three fields: a pre-pass it interrupted (newConw 0)
+// runs again from the start, which ends at the same conw_r).  On restart the
+// scan resumes at nlines + 1 and the output is appended.
 // Exit codes follow the reference: -1 missing input, 1 output cannot be
 // opened, 2 limit exceeded / malformed input, 4 singular ellipsoid fit.
 #include <cstdio>

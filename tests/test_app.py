@@ -1,9 +1,13 @@
 """The drop-in executable periodsearch_b200/period_search_b200: the
 reference's file contract (period_search_in -> period_search_out, in the
 reference's 6-column format), checkpoint/resume through period_search_state
-(the CUDA application's "nlines newConw conw_r" form and the CPU
-application's bare "nlines", which re-runs the convexity pre-pass), and the
-reference's exit codes."""
+(the CUDA application's "nlines newConw conw_r" form, the CPU application's
+bare "nlines", which re-runs the convexity pre-pass, and the five-field
+"nlines newConw conw_r sum_dark_facet ntestperiods" form of the pure-CPU and
+OpenCL applications, period_search_pure_cpu_win/period_search/
+period_search_BOINC.cpp:91,257, whose first three fields are read and whose
+interrupted pre-pass is run again from the start), and the reference's exit
+codes."""
 import os
 import shutil
 import subprocess
@@ -47,7 +51,7 @@ def test_executable_matches_reference_output(native, tmp_path, name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("state_form", ["cuda", "cpu"])
+@pytest.mark.parametrize("state_form", ["cuda", "cpu", "five", "five_prepass"])
 def test_executable_resumes_from_checkpoint(native, tmp_path, state_form):
     shutil.copy(golden_path("tiny"), tmp_path / "period_search_in")
     full = tmp_path / "full"
@@ -56,10 +60,15 @@ def test_executable_resumes_from_checkpoint(native, tmp_path, state_form):
     assert _run(full).returncode == 0
     whole = (full / "period_search_out").read_text().splitlines(True)
     state = (full / "period_search_state").read_text().split()
-    # interrupted after two periods
-    (tmp_path / "period_search_out").write_text("".join(whole[:2]))
+    # interrupted after two periods (or, five_prepass, during the pre-pass)
+    done = 0 if state_form == "five_prepass" else 2
+    (tmp_path / "period_search_out").write_text("".join(whole[:done]))
     if state_form == "cuda":
         (tmp_path / "period_search_state").write_text("2 1 %s" % state[2])
+    elif state_form == "five":
+        (tmp_path / "period_search_state").write_text("2 1 %s 3.5 10" % state[2])
+    elif state_form == "five_prepass":
+        (tmp_path / "period_search_state").write_text("0 0 %s 1.25 3" % state[2])
     else:
         (tmp_path / "period_search_state").write_text("2")
     r = _run(tmp_path, "--chunk", "1")
