@@ -480,11 +480,13 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
         tk[i] = kt * 8;
         acc[i][0] = acc[i][1] = 0;
     }
+    // warp w copies parameter columns w, w + 8, ...; lane r rows r, r + 32, ...
     auto issue = [&](int r0, int b) {
         const int nr = min(rt, nrows - r0);
-        for (int idx = tid; idx < nr * mfit; idx += kThreads) {
-            const int j = idx / nr, r = idx - j * nr;
-            cp_async8(work + b * bstride + r * st + j, Jt + (size_t)P.free_idx[j] * npad + r0 + r);
+        for (int j = warp; j < mfit; j += kThreads / 32) {
+            const double* src = Jt + (size_t)P.free_idx[j] * npad + r0;
+            double* dst = work + b * bstride + j;
+            for (int r = lane; r < nr; r += 32) cp_async8(dst + r * st, src + r);
         }
         cp_async_commit();
     };
