@@ -568,7 +568,7 @@ def main():
                    "fits_per_step": fits_per_step, "l2": "flushed (256 MB write) between timed steps",
                    "prepass": {"fits": None, "seconds": prepass_s, "conw_r": conw_r},
                    "tiles": {"fch": tiles[0], "rt": tiles[1], "sortseg": tiles[2], "chosen_by": "ps_autotune"}
-                   if tiles else "defaults (32, 32, 1024)",
+                   if tiles else "defaults (40, 32, 1024)",
                    "parallelism": f"period shards x{world}"},
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),

@@ -200,11 +200,11 @@ int ps_format_record(const ps_record* r, int first_line, double conw_line, char*
  * number of points sorted together by viewing direction (sortseg, a power
  * of 2, 32..4096) in both FP64 forms.  No choice changes any result (the
  * sums keep their order); they change speed and shared memory.  Defaults
- * 32, 32, 1024.  PS_ERR_LIMIT if the layout does not fit.  No counterpart
+ * 40, 32, 1024.  PS_ERR_LIMIT if the layout does not fit.  No counterpart
  * in the reference (fixed array sizes there).
  * ps_autotune: time scans of trial periods 1..n (n = n_periods, at least
  * two waves of fits: 4 x SMs / 10 periods) under candidate
- * tiles (fch, rt in {16, 32, 64}; sortseg in {256, 1024}; the
+ * tiles (fch in {16, 32, 40, 48, 64}, rt in {16, 32, 64}; sortseg in {256, 1024}; the
  * reference-order form only sortseg), keep the fastest; tiles[3] and
  * *seconds (its scan time) receive the choice. */
 int ps_set_tiles(ps_ctx* ctx, int fch, int rt, int sortseg);

@@ -354,7 +354,7 @@ class PeriodSearchBatch:
         k = int(order[np.searchsorted(np.cumsum(work[order]), 0.5 * work.sum())])
         tuned, _ = ctxs[k].autotune(n_periods)
         best, tbest = None, None
-        for tiles in dict.fromkeys([(32, 32, 1024), tuple(tuned)]):
+        for tiles in dict.fromkeys([(40, 32, 1024), tuple(tuned)]):
             for c in ctxs:
                 c.set_tiles(*tiles)
             b = PeriodSearchBatch(ctxs)

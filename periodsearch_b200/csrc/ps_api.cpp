@@ -244,7 +244,7 @@ int upload_static(ps_ctx* c) {
     d.cpl = c->d_cpl.p;
     d.cfc = c->d_cfc.p;
     d.cfs = c->d_cfs.p;
-    d.fch = 32;
+    d.fch = 40;  // the largest chunk that keeps two c2-size fits (C = 49, mfit = 55) per SM
     d.rt = 32;
     d.sortseg = 1024;
     d.cg_first = c->d_cgf.p;
@@ -605,7 +605,7 @@ int ps_autotune(ps_ctx* c, int n_periods, int* tiles, double* seconds) {
     if (rc) return rc;
     int best[3] = {start[0], start[1], start[2]};
     double tbest = 1e300;
-    static const int fchs[] = {16, 32, 64}, rts[] = {16, 32, 64}, segs[] = {256, 1024};
+    static const int fchs[] = {16, 32, 40, 48, 64}, rts[] = {16, 32, 64}, segs[] = {256, 1024};
     for (int fch : fchs)
         for (int rt : rts)
             for (int seg : segs) {
