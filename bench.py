@@ -35,7 +35,10 @@ import time
 REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
-METRIC = "converged LM fits/sec on 1 B200: mixed+batched vs FP64 GPU at matched chi2"
+# what the line measures: LM fits (trial period x initial pole, each run to
+# the reference's stop rule) per second; the form that produced `value` is
+# config.form, and `forms` holds the other forms timed on the same batch
+METRIC = "converged LM fits/sec on 1 B200 (reference stop rule)"
 WORKLOAD = ("c2 production sparse search: N=760 (600 sparse + 2x80 dense), lmax=mmax=6 (C=49), nrows=10 (F=800), "
             "50 LM iterations/fit, 2-100 h at step coef 2.15 (39153 periods) x 10 poles")
 
@@ -398,6 +401,7 @@ def main():
                     help="fast: FP64 with the shape block on FP64 tensor cores (the headline); fp64: reference operation order")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip timing the other numerical forms on one batch")
     ap.add_argument("--config", default="c2", choices=["c2", "c4", "c5"],
                     help="c2: production sparse search (the headline); c4: uneven multi-asteroid batch; "
                          "c5: lmax 8 / 2048 facets / 20000 points (14 periods per step, no pre-pass)")
@@ -412,7 +416,7 @@ def main():
         args.periods_per_step = min(args.periods_per_step, 14)
     if args.profile:
         args.periods_per_step = 30
-        args.no_cpu = args.no_e2e = True
+        args.no_cpu = args.no_e2e = args.no_forms = True
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -471,9 +475,18 @@ def main():
     d_rec = torch.zeros(B * 6, dtype=torch.float64, device="cuda")
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
+    # the product's period partition (periodsearch_b200.shard): blocks of B
+    # consecutive trial periods dealt round-robin over the ranks; a rank's
+    # steps walk through its own full blocks (and start over on a long run),
+    # so ranks never scan the same periods
+    from periodsearch_b200.shard import period_blocks
+
+    blocks = [blk for blk in period_blocks(n_total, world, rank, B) if blk[1] - blk[0] + 1 == B]
+    if not blocks:
+        raise SystemExit(f"fewer than {B * world} trial periods for {world} ranks")
+
     def batch(step):
-        first = 1 + ((step * world + rank) * B) % max(n_total - B, 1)
-        return first, first + B - 1
+        return blocks[step % len(blocks)]
 
     for s in range(args.warmup):
         a, b = batch(s)
@@ -501,23 +514,75 @@ def main():
     value = world * fits_per_step * args.steps / t_max
     clocks = clk.summary()
 
-    # e2e through the public API from host buffers
+    # e2e through the public API from host buffers: per step, open a context
+    # from the caller's host arrays (host setup, uploads), set conw_r, scan
+    # the step's periods into host records, close.  The timed e2e steps scan
+    # the same period batches as the first device-timed steps, so the two
+    # can be compared batch for batch; one untimed e2e call on a warm-up
+    # batch comes first.
     rec_host = np.zeros(B, dtype=ps.RECORD_DTYPE)
-    e2e_times = []
     desc = _desc_from(g, path)
     h2d = sum(np.asarray(v).nbytes for v in desc.values() if isinstance(v, np.ndarray))
-    for s in range(0 if args.no_e2e else min(args.steps, 3) + 1):
+    n_e2e = 0 if args.no_e2e else min(args.steps, 5)
+    e2e_times, phases = [], {"open": [], "set_conw_r": [], "scan": [], "close": []}
+    for s in range(-1, n_e2e):
         a, b = batch(args.warmup + s)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         h = ps.PeriodSearch(desc=desc, device=local, form=form)
+        t1 = time.perf_counter()
         h.set_conw_r(conw_r)
+        t2 = time.perf_counter()
         rec_host = h.scan(a, b)
+        t3 = time.perf_counter()
         h.close()
-        dt = time.perf_counter() - t0
-        if s:
-            e2e_times.append(dt)
+        t4 = time.perf_counter()
+        if s >= 0:
+            e2e_times.append(t4 - t0)
+            for k, dt in zip(phases, (t1 - t0, t2 - t1, t3 - t2, t4 - t3)):
+                phases[k].append(dt)
     e2e_value = world * fits_per_step * len(e2e_times) / sum(e2e_times) if e2e_times else None
+    same = times[:len(e2e_times)]
+    e2e_extra = {"device_same_batches": world * fits_per_step * len(same) / sum(same) if same else None,
+                 "phase_ms_median": {k: 1000 * statistics.median(v) for k, v in phases.items() if v},
+                 "steps": len(e2e_times)}
+
+    # the other numerical forms on the first timed batch (same periods, same
+    # L2 flush, device-resident), with their per-period chi2 difference to
+    # this run's records of that batch
+    forms = {}
+    if not args.no_forms and world == 1:
+        a0, b0 = batch(args.warmup)
+        g.scan_device(a0, b0, d_rec.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        base = d_rec.view(B, 6).cpu().numpy().copy()
+        own_s = times[0]
+        for other in [f for f in ("fp64", "fast", "mixed") if f != args.form]:
+            if other == "mixed" and g.ncoef > 64:
+                forms[other] = {"unavailable": "the mixed form holds at most 64 shape coefficients"}
+                continue
+            h = ps.PeriodSearch(path, device=local, form={"fp64": ps.PS_FORM_FP64, "fast": ps.PS_FORM_FAST,
+                                                           "mixed": ps.PS_FORM_MIXED}[other])
+            h.set_conw_r(conw_r)
+            h.scan_device(a0, a0 + 29, d_rec.data_ptr(), stream.cuda_stream)  # warm-up
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            h.scan_device(a0, b0, d_rec.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            t_o = e0.elapsed_time(e1) / 1000.0
+            rec_o = d_rec.view(B, 6).cpu().numpy()
+            rel = np.abs(rec_o[:, 2] - base[:, 2]) / np.abs(base[:, 2])
+            top = lambda r, k: list(np.argsort(r[:, 2], kind="stable")[:k])
+            forms[other] = {"fits_per_s": fits_per_step / t_o, "ratio_of_this_form_to_it": t_o / own_s,
+                            "chi2_rel_diff_to_this_form": {"median": float(np.median(rel)),
+                                                           "p90": float(np.quantile(rel, 0.9)),
+                                                           "max": float(rel.max())},
+                            "same_top1_10_20": [top(rec_o, k) == top(base, k) for k in (1, 10, 20)]}
+            h.close()
 
     # check a few records of the last timed batch against the same call again
     got = d_rec.view(B, 6).cpu().numpy()
@@ -566,15 +631,17 @@ def main():
         "data": "synthetic",
         "config": {"workload": WORKLOAD_C5 if args.config == "c5" else WORKLOAD, "form": {"fp64": "fp64 (drop-in, reference operation order)", "fast": "fast fp64 (rearranged, fused; rounding-level differences)", "mixed": "mixed (FP64 model/solve, FP32 derivatives, tcgen05 split-BF16 shape block)"}[args.form], "periods_per_step": B,
                    "fits_per_step": fits_per_step, "l2": "flushed (256 MB write) between timed steps",
-                   "prepass": {"fits": None, "seconds": prepass_s, "conw_r": conw_r},
+                   "prepass": {"fits": getattr(g, "prepass_fits", 0), "seconds": prepass_s, "conw_r": conw_r,
+                               "fits_per_s": (getattr(g, "prepass_fits", 0) / prepass_s) if prepass_s else None},
                    "tiles": {"fch": tiles[0], "rt": tiles[1], "sortseg": tiles[2], "chosen_by": "ps_autotune"}
                    if tiles else "defaults (40, 32, 1024)",
                    "parallelism": f"period shards x{world}"},
         "roofline": roofline,
         "e2e": {"value": e2e_value, "unit": "fits/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(rec_host.nbytes)},
+                "d2h_bytes_per_step": int(rec_host.nbytes), **e2e_extra},
         "gpu_launches": int(launches),
         "clocks": clocks,
+        "forms": forms or None,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         r, why = ref_cpu_sample_or_none(path, 1)

@@ -105,8 +105,13 @@ int ps_open_file(const char* path, int device, int form, ps_ctx** out);
 /* Same from in-memory arrays (replaces CUDAPrepare + the host globals). */
 int ps_open(const ps_problem_desc* desc, int device, int form, ps_ctx** out);
 /* Release the context and its device memory (replaces CUDAUnprepare,
- * start_CUDA.h:14). */
+ * start_CUDA.h:14).  The context's large Jacobian work buffer goes back to a
+ * per-device cache (a few buffers per device) for the next context, so that
+ * opening a context per asteroid does not allocate and free it every time. */
 void ps_close(ps_ctx* ctx);
+/* Free the cached work buffers of every device.  No counterpart in the
+ * reference (its buffers are static arrays). */
+void ps_release_cached_memory(void);
 
 /* Convexity-weight optimisation pre-pass (replaces CUDAPrecalc,
  * start_CUDA.h:9-10; period_search_BOINC.cpp:487-715), then the final setup
@@ -123,22 +128,31 @@ int ps_n_periods(const ps_ctx* ctx);
  * formats the lines).  Requires ps_precalc or ps_set_conw_r first. */
 int ps_scan(ps_ctx* ctx, int n_from, int n_to, ps_record* out);
 /* Same, but the records stay on the device: d_out is a device pointer to
- * (n_to - n_from + 1) records; stream is a cudaStream_t (NULL = default).
- * Used to time the scan with inputs and outputs resident in HBM. */
+ * (n_to - n_from + 1) records; stream is a cudaStream_t (NULL = the
+ * context's own stream, not the legacy default stream); asynchronous.  The
+ * context's tables are complete on the device when ps_open* and
+ * ps_precalc / ps_set_conw_r return, so any stream may scan afterwards.
+ * Scans of one context share its work buffers: scans on different streams
+ * must not overlap on the GPU. */
 int ps_scan_device(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, void* stream);
 
 /* ps_scan_device without any device-memory allocation.  No counterpart in
- * the reference: it exists for callers that cannot allocate while they scan
- * (work recorded into a CUDA graph, a fixed pre-sized memory budget, a plugin
- * inside a process whose allocator it does not own).  Set the context up
- * first (ps_open*, then ps_precalc or ps_set_conw_r, which allocate); this
- * call then takes all scratch from one 64 MiB device array that the library
- * holds on every GPU it runs on until exit, and rejects, with PS_ERR_LIMIT, a
- * period range whose 72 bytes per fit plus one CTA's Jacobian scratch do not
- * fit in it.  Asynchronous on `stream` (NULL = the context's stream).  All
- * calls share the array: calls that overlap on the GPU race, so serialise
- * them.  The first call on a device looks up the array's device address;
- * make it before any stream capture.  FP64 form only. */
+ * the reference.  It is for callers that cannot allocate device memory while
+ * they scan: a host that gives this library a fixed device-memory budget up
+ * front, a plugin running inside a process whose allocator it does not own,
+ * or a latency-sensitive service for which cudaMalloc/cudaFree are not
+ * acceptable on the scan path (cudaFree waits for the whole device).  Set the
+ * context up first (ps_open*, then ps_precalc or ps_set_conw_r, which
+ * allocate the per-asteroid tables); this call then takes all scratch from
+ * one 64 MiB device array that the library holds on every GPU it runs on
+ * until exit, and rejects, with PS_ERR_LIMIT, a period range whose 72 bytes
+ * per fit plus one CTA's Jacobian scratch do not fit in it.  Asynchronous on
+ * `stream` (NULL = the context's stream).  All calls share the array and it
+ * keeps the last call's contents: calls that overlap on the GPU race, so
+ * serialise them.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress); make that first call before any stream
+ * capture begins.  FP64 form only; that form has no bounded
+ * device wait, so there is no device error word to check afterwards. */
 int ps_scan_device_noalloc(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, void* stream);
 
 /* Batched scans: many asteroids in one persistent launch, each fit pulling
@@ -175,7 +189,8 @@ int ps_mrqcof(ps_ctx* ctx, const double* a, double* alpha, double* beta, double*
 int ps_model(ps_ctx* ctx, const double* a, double* ymod, double* dyda);
 
 /* Sizes: [0] n_points, [1] n_lc (incl. convexity pseudo-curve),
- * [2] numfac, [3] ncoef, [4] ma, [5] mfit, [6] n_periods.
+ * [2] numfac, [3] ncoef, [4] ma, [5] mfit, [6] n_periods, [7] fits run by
+ * the last ps_precalc (10 poles x up to 10 periods per pre-pass round).
  * Scalars: [0] escl, [1] conw_r, [2] freq_start, [3] freq_end,
  * [4] freq_step. */
 int ps_info(const ps_ctx* ctx, int* ints, double* dbls);

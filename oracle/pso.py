@@ -17,7 +17,8 @@ LIB = os.path.join(HERE, "libps_oracle.so")
 EXE = os.path.join(HERE, "ps_oracle")
 REF_EXE = os.path.join(HERE, "_ref", "period_search_ref")
 REF_FMA_EXE = os.path.join(HERE, "_ref", "period_search_ref_fma")
-REF_SRC = "/root/reference/period_search"
+# where the reference checkout lies (set PS_REFERENCE_DIR to move it)
+REF_SRC = os.path.join(os.environ.get("PS_REFERENCE_DIR", "/root/reference"), "period_search")
 
 RECORD_DTYPE = np.dtype(
     [("period_h", "f8"), ("rms", "f8"), ("chi2", "f8"), ("dark_pct", "f8"), ("lambda_deg", "f8"), ("beta_deg", "f8")]

@@ -116,6 +116,7 @@ EXPORTS = (
     "ps_format_record", "ps_last_error", "ps_kernel_launches", "ps_scan_device_noalloc",
     "ps_batch_open", "ps_batch_scan", "ps_batch_scan_device", "ps_batch_fit_cycles", "ps_batch_close",
     "ps_fp64_tensor_peak", "ps_chi2_grad", "ps_gn_product", "ps_set_tiles", "ps_autotune",
+    "ps_release_cached_memory",
 )
 
 
@@ -158,6 +159,7 @@ def load_library(path: str | None = None):
         "ps_set_tiles": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
         "ps_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _D]),
         "ps_gn_product": (ctypes.c_int, [vp, _D, _D, _D]),
+        "ps_release_cached_memory": (None, []),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -222,6 +224,9 @@ class PeriodSearch:
         v = ctypes.c_double()
         _check(self._lib.ps_precalc(self._h, ctypes.byref(v)))
         self.conw_r = v.value
+        ints = (ctypes.c_int * 8)()
+        self._lib.ps_info(self._h, ints, None)
+        self.prepass_fits = ints[7]
         return v.value
 
     def set_conw_r(self, conw_r: float):

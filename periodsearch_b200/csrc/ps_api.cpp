@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -41,6 +42,57 @@ int cuda_fail(cudaError_t e, const char* where) {
 namespace psb {
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
 void count_launch() { g_launches++; }
+
+namespace {
+struct PoolEntry {
+    int device;
+    void* p;
+    size_t cap;
+};
+std::mutex g_pool_mu;
+std::vector<PoolEntry> g_pool;
+constexpr int kPoolPerDevice = 4;
+}  // namespace
+
+cudaError_t pool_take(int device, size_t bytes, void** p, size_t* cap) {
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        int best = -1;
+        for (int i = 0; i < (int)g_pool.size(); i++)
+            if (g_pool[i].device == device && g_pool[i].cap >= bytes && (best < 0 || g_pool[i].cap < g_pool[best].cap))
+                best = i;
+        if (best >= 0) {
+            *p = g_pool[best].p;
+            *cap = g_pool[best].cap;
+            g_pool.erase(g_pool.begin() + best);
+            return cudaSuccess;
+        }
+    }
+    *p = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaSuccess) *cap = bytes;
+    return e;
+}
+
+void pool_give(int device, void* p, size_t cap) {
+    void* drop = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        g_pool.push_back({device, p, cap});
+        int count = 0, smallest = -1;
+        for (int i = 0; i < (int)g_pool.size(); i++)
+            if (g_pool[i].device == device) {
+                count++;
+                if (smallest < 0 || g_pool[i].cap < g_pool[smallest].cap) smallest = i;
+            }
+        if (count > kPoolPerDevice) {
+            drop = g_pool[smallest].p;
+            g_pool.erase(g_pool.begin() + smallest);
+        }
+    }
+    if (drop) cudaFree(drop);
+}
 }  // namespace psb
 
 namespace {
@@ -304,6 +356,11 @@ int upload_rows(ps_ctx* c) {
     c->dp.conw_r = p.conw_r;
     PSB_CUDA(c->d_dp.ensure(1));
     PSB_CUDA(cudaMemcpyAsync(c->d_dp.p, &c->dp, sizeof(psb::DevProblem), cudaMemcpyHostToDevice, c->stream));
+    // The copies above are from pageable host memory: the call may return
+    // before the device holds the data.  A scan launched later on a caller's
+    // stream is not ordered after the context's own stream, so the tables
+    // must be in place before this returns.
+    PSB_CUDA(cudaStreamSynchronize(c->stream));
     c->rows_ready = true;
     return PS_OK;
 }
@@ -314,7 +371,7 @@ size_t scratch_stride(const ps_ctx* c) {
 
 int ensure_scratch(ps_ctx* c, int slots) {
     const size_t stride = scratch_stride(c);
-    PSB_CUDA(c->d_scratch.ensure(stride * slots));
+    PSB_CUDA(c->d_scratch.ensure(c->device, stride * slots));
     return PS_OK;
 }
 
@@ -362,6 +419,7 @@ int open_device(ps_ctx* c, int device) {
     c->host_only = false;
     int rc = upload_static(c);
     if (rc) return rc;
+    PSB_CUDA(cudaStreamSynchronize(c->stream));  // tables in place before any caller stream uses them
     return PS_OK;
 }
 
@@ -377,6 +435,21 @@ int check_ready(const ps_ctx* c, bool need_rows) {
 extern "C" {
 
 const char* ps_last_error(void) { return g_err.c_str(); }
+
+void ps_release_cached_memory(void) {
+    std::vector<psb::PoolEntry> all;
+    {
+        std::lock_guard<std::mutex> lk(psb::g_pool_mu);
+        all.swap(psb::g_pool);
+    }
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (const auto& e : all) {
+        cudaSetDevice(e.device);
+        cudaFree(e.p);
+    }
+    cudaSetDevice(cur);
+}
 long long ps_kernel_launches(void) { return g_launches.load(); }
 
 int ps_open_host_only(const char* path, ps_ctx** out) {
@@ -493,7 +566,7 @@ void ps_close(ps_ctx* c) {
         c->d_lc.release();
         c->d_free.release();
         c->d_queue.release();
-        c->d_scratch.release();
+        c->d_scratch.release(c->device);
         c->d_fits.release();
         c->d_rec.release();
         c->d_eval.release();
@@ -513,6 +586,7 @@ int ps_precalc(ps_ctx* c, double* conw_r) {
     PSB_CUDA(cudaSetDevice(c->device));
     Problem& p = c->prob;
     int new_conw = 0;
+    c->prepass_fits = 0;
     std::vector<ps_record> rec(10);
     // period_search_BOINC.cpp:488-715
     while ((new_conw != 1) && ((p.conw_r * p.escl * p.escl) < 10.0)) {
@@ -525,6 +599,7 @@ int ps_precalc(ps_ctx* c, double* conw_r) {
         PSB_CUDA(c->d_rec.ensure(10));
         rc = scan_into(c, 1, max_test_periods, c->d_rec.p, 1);
         if (rc) return rc;
+        c->prepass_fits += 10 * max_test_periods;
         PSB_CUDA(cudaMemcpyAsync(rec.data(), c->d_rec.p, sizeof(ps_record) * max_test_periods,
                                  cudaMemcpyDeviceToHost, c->stream));
         PSB_CUDA(cudaStreamSynchronize(c->stream));
@@ -804,6 +879,7 @@ int ps_info(const ps_ctx* c, int* ints, double* dbls) {
         ints[4] = p.ma;
         ints[5] = p.mfit;
         ints[6] = p.n_periods();
+        ints[7] = c->prepass_fits;
     }
     if (dbls) {
         dbls[0] = p.escl;

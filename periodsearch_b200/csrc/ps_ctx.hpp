@@ -44,6 +44,38 @@ struct DevBuf {
     }
 };
 
+// Process-wide cache of large device work buffers per device.  A context
+// borrows one for its Jacobian scratch and returns it when it closes, so
+// that opening and closing a context per asteroid does not pay a cudaMalloc
+// and a device-synchronising cudaFree of ~100 MB each time.  A buffer
+// belongs to one context at a time; at most a few buffers per device stay
+// cached, until ps_release_cached_memory or process exit.
+cudaError_t pool_take(int device, size_t bytes, void** p, size_t* cap);
+void pool_give(int device, void* p, size_t cap);
+
+template <class T>
+struct PooledBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaError_t ensure(int device, size_t count) {
+        if (count <= n) return cudaSuccess;
+        release(device);
+        void* q = nullptr;
+        size_t cap = 0;
+        cudaError_t e = pool_take(device, count * sizeof(T), &q, &cap);
+        if (e == cudaSuccess) {
+            p = (T*)q;
+            n = cap / sizeof(T);
+        }
+        return e;
+    }
+    void release(int device) {
+        if (p) pool_give(device, p, n * sizeof(T));
+        p = nullptr;
+        n = 0;
+    }
+};
+
 }  // namespace psb
 
 struct ps_ctx {
@@ -54,11 +86,12 @@ struct ps_ctx {
     bool rows_ready = false;
     cudaStream_t stream = nullptr;
     int sms = 0, blocks_per_sm = 0;
+    int prepass_fits = 0;  // fits run by the last ps_precalc
     psb::DevProblem dp{};
     // device tables
     psb::DevBuf<double> d_pts, d_rows, d_fac, d_dsph, d_cpl, d_cfc, d_cfs, d_cgf, d_pole;
     psb::DevBuf<int> d_lc, d_free, d_queue;
-    psb::DevBuf<double> d_scratch;
+    psb::PooledBuf<double> d_scratch;
     psb::DevBuf<psb::FitOut> d_fits;
     psb::DevBuf<ps_record> d_rec;
     psb::DevBuf<double> d_eval;

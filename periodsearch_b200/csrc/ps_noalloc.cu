@@ -3,9 +3,10 @@
 // file-scope device array instead of from cudaMalloc.
 //
 // Who needs this: callers that must not allocate device memory while they
-// run -- code that records the scan into a CUDA graph it replays later, a
-// host that runs under a fixed, pre-sized device-memory budget, or a plugin
-// loaded into a process whose allocator it does not own.  Such a caller sets
+// run -- a host that runs under a fixed, pre-sized device-memory budget, a
+// plugin loaded into a process whose allocator it does not own, or a
+// latency-sensitive service that cannot take cudaMalloc/cudaFree on its scan
+// path (cudaFree waits for all work on the device).  Such a caller sets
 // the context up once (ps_open*, ps_precalc / ps_set_conw_r allocate the
 // per-asteroid tables there) and afterwards scans with this entry point,
 // which calls no cudaMalloc, cudaFree or other allocating routine.

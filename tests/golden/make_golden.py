@@ -49,7 +49,7 @@ REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
 sys.path.insert(0, os.path.join(REPO, "oracle"))
 
-REF_ROOT = "/root/reference"
+REF_ROOT = os.environ.get("PS_REFERENCE_DIR", "/root/reference")
 REF_EXE = os.path.join(REPO, "oracle", "_ref", "period_search_ref")
 REF_FMA = os.path.join(REPO, "oracle", "_ref", "period_search_ref_fma")
 

@@ -84,3 +84,39 @@ def test_executable_exit_codes(native, tmp_path):
     (tmp_path / "period_search_in").write_text("90 0.5 100 1\n0\n")
     r = _run(tmp_path)
     assert r.returncode == 2
+
+
+@pytest.mark.gpu
+def test_sharded_scan_merges_to_the_unsharded_output(native, tmp_path):
+    """Two shards run one after the other on one GPU (--shard 0/2, 1/2, in
+    blocks of 7 periods), one of them interrupted and resumed, then --merge 2:
+    period_search_out and period_search_state equal the unsharded run's
+    byte for byte."""
+    full = tmp_path / "full"
+    full.mkdir()
+    shutil.copy(golden_path("c1"), full / "period_search_in")
+    r = _run(full, "--chunk", "7")
+    assert r.returncode == 0, r.stderr
+    d = tmp_path / "sharded"
+    d.mkdir()
+    shutil.copy(golden_path("c1"), d / "period_search_in")
+    for k in (0, 1):
+        r = _run(d, "--shard", f"{k}/2", "--chunk", "7")
+        assert r.returncode == 0, r.stderr
+    # incomplete shards are refused: drop shard 1's last block and its state
+    s1 = d / "period_search_out.shard_1_of_2"
+    st1 = d / "period_search_state.shard_1_of_2"
+    whole1 = s1.read_text()
+    lines = whole1.splitlines(True)
+    s1.write_text("".join(lines[:-7] if len(lines) > 8 else lines))
+    done, newc, cw = st1.read_text().split()
+    st1.write_text("%d %s %s" % (int(done) - 1, newc, cw))
+    assert _run(d, "--merge", "2").returncode == 2
+    # resume the interrupted shard, then merge
+    r = _run(d, "--shard", "1/2", "--chunk", "7")
+    assert r.returncode == 0, r.stderr
+    assert s1.read_text() == whole1
+    r = _run(d, "--merge", "2")
+    assert r.returncode == 0, r.stderr
+    assert (d / "period_search_out").read_text() == (full / "period_search_out").read_text()
+    assert (d / "period_search_state").read_text() == (full / "period_search_state").read_text()

@@ -1,6 +1,7 @@
 """ps_scan_device_noalloc: the period scan for callers that cannot allocate
-device memory while they run (work recorded into a CUDA graph, a fixed
-pre-sized memory budget, a plugin inside someone else's process).  It must
+device memory while they run (a fixed pre-sized memory budget, a plugin
+inside someone else's process, a service that cannot take cudaFree's
+device-wide wait on its scan path).  It must
 give the same records as ps_scan_device, call after call, with all of its
 scratch in the library's fixed 64 MiB device array, and refuse a request that
 does not fit there.  This file is collected last on purpose."""
@@ -16,10 +17,10 @@ from conftest import golden_path
 pytestmark = pytest.mark.gpu
 
 
-def _records(torch, ps, fn, g, n_from, n_to):
+def _records(torch, ps, fn, g, n_from, n_to, stream=None):
     n = n_to - n_from + 1
     d = torch.full((n * 6,), float("nan"), dtype=torch.float64, device="cuda")
-    rc = fn(g._h, n_from, n_to, ctypes.c_void_p(d.data_ptr()), None)
+    rc = fn(g._h, n_from, n_to, ctypes.c_void_p(d.data_ptr()), stream)
     assert rc == ps.PS_OK, ps.load_library().ps_last_error()
     torch.cuda.synchronize()
     return d.view(n, 6).cpu().numpy()
@@ -43,6 +44,26 @@ def test_noalloc_scan_matches_scan_device(native):
     again = _records(torch, ps, lib.ps_scan_device_noalloc, g, 11, 40)
     np.testing.assert_allclose(again, ref, rtol=1e-12, atol=0)
     g.close()
+
+
+def test_noalloc_on_caller_stream_right_after_setup(native):
+    """A caller's own stream, used straight after ps_set_conw_r returns: the
+    scan must see the tables that call uploaded (no ordering with the
+    context's internal stream is needed)."""
+    torch = pytest.importorskip("torch")
+    ps = native
+    lib = ps.load_library()
+    g = ps.PeriodSearch(golden_path("c1"))
+    g.set_conw_r(g.conw_r * 8)
+    ref = _records(torch, ps, lib.ps_scan_device, g, 11, 40)
+    g.close()
+    s = torch.cuda.Stream()
+    for _ in range(2):
+        g = ps.PeriodSearch(golden_path("c1"))
+        g.set_conw_r(g.conw_r * 8)
+        got = _records(torch, ps, lib.ps_scan_device_noalloc, g, 11, 40, ctypes.c_void_p(s.cuda_stream))
+        np.testing.assert_allclose(got, ref, rtol=1e-12, atol=0)
+        g.close()
 
 
 def test_noalloc_rejects_oversized_request(native, tmp_path):
