@@ -318,11 +318,14 @@ def run_c4(args, local):
         made = pool.map(_c4_worker, [(i, workdir) for i in range(args.asteroids)])
     torch.cuda.set_device(local)
     form = {"fp64": ps.PS_FORM_FP64, "fast": ps.PS_FORM_FAST}[args.form]
-    ctxs = []
-    for p, _ in made:
-        c = ps.PeriodSearch(p, device=local, form=form)
-        c.set_conw_r(c.conw_r)
-        ctxs.append(c)
+    # per-asteroid host setup + uploads: on host threads (the product's
+    # open_many), timed; one asteroid on one thread for comparison
+    t0 = time.perf_counter()
+    ctxs = ps.open_many([p for p, _ in made], device=local, form=form, conw_r="start")
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    ps.open_many([made[0][0]], device=local, form=form, conw_r="start", threads=1)[0].close()
+    setup_one_s = time.perf_counter() - t0
     P = args.c4_periods
     n_per = np.array([c.n_periods for c in ctxs])
     tiles = None
@@ -345,7 +348,7 @@ def run_c4(args, local):
         batch.scan_device(a, b, d_rec.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
     launches0 = ps.load_library().ps_kernel_launches()
-    times, fits, cycles = [], 0, None
+    times, fits, busy, done = [], 0, None, None
     with ClockSampler(local) as clk:
         for s in range(args.steps):
             flush.zero_()
@@ -359,11 +362,9 @@ def run_c4(args, local):
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1000.0)
             fits += int(10 * (b - a + 1).sum())
-            cycles = batch.fit_cycles()
+            busy, done = batch.fit_times()
     launches = ps.load_library().ps_kernel_launches() - launches0
     clocks = clk.summary()
-    hz = (clocks.get("sm_mhz") or 1965.0) * 1e6
-    per_ast = cycles / hz
     value = fits / sum(times)
     line = {
         "metric": METRIC + " (uneven batch)", "value": value, "unit": "fits/s", "n_gpus": 1, "steps": args.steps,
@@ -377,16 +378,90 @@ def run_c4(args, local):
                               "chosen_by": "PeriodSearchBatch.autotune (ps_autotune on the work-weighted "
                                            "median asteroid, checked against the defaults on one batch scan)"}
                              if tiles else "defaults"),
-                   "l2": "flushed (256 MB write) between timed steps"},
-        "per_asteroid_ms": {"p50": 1000 * float(np.percentile(per_ast, 50)),
-                            "p99": 1000 * float(np.percentile(per_ast, 99)),
-                            "what": "SM-time of one asteroid's fits in the last step (sum over its fits of "
-                                    "the fit's clock cycles / SM clock)"},
+                   "l2": "flushed (256 MB write) between timed steps",
+                   "setup": {"seconds": setup_s, "asteroids": len(ctxs), "threads": min(len(made), os.cpu_count() or 1, 32),
+                             "one_asteroid_s": setup_one_s,
+                             "what": "host setup + uploads of every asteroid (ps.open_many), not in the timed steps"}},
+        "per_asteroid_ms": {"p50": float(np.percentile(done, 50)), "p99": float(np.percentile(done, 99)),
+                            "max": float(np.max(done)),
+                            "what": "wall latency of one asteroid in the last timed step: from the start of the "
+                                    "step's first fit to the end of the asteroid's last fit (GPU global timer)",
+                            "busy_p50": float(np.percentile(busy, 50)), "busy_p99": float(np.percentile(busy, 99)),
+                            "busy_what": "summed duration of the asteroid's fits (fits run in parallel)"},
         "gpu_launches": int(launches), "clocks": clocks,
     }
     batch.close()
     for c in ctxs:
         c.close()
+    print(json.dumps(line), flush=True)
+
+
+def initial_parameters(g, freq, pole):
+    """cg at the start of fit (freq, pole), period_search_BOINC.cpp:819-844,
+    from the context's own host tables."""
+    import numpy as np
+
+    beta_pole = [0, 0, 0, 0, 60, 60, 60, -60, -60, -60]
+    lambda_pole = [0, 90, 180, 270, 60, 180, 300, 60, 180, 300]
+    C = g.ncoef
+    a = np.zeros(g.ma)
+    a[:C] = g.array("cg_first")
+    a[C] = np.radians(90.0 - beta_pole[pole - 1])
+    a[C + 1] = np.radians(lambda_pole[pole - 1])
+    a[C + 2] = 24 * 2 * np.pi * freq
+    return a
+
+
+def run_adjoint(args, path, local):
+    """Matrix-free Gauss-Newton products J^T W (J v) (ps_gn_product) at the
+    workload's size: products per second through the C ABI (parameters and
+    direction uploaded, result read back per call), with the FLOP count of
+    one product, 4 N F C (two passes over the (point, facet) pairs, two F x C
+    contractions)."""
+    import numpy as np
+    import torch
+
+    import periodsearch_b200 as ps
+
+    torch.cuda.set_device(local)
+    g = ps.PeriodSearch(path, device=local, form=ps.PS_FORM_FAST)
+    g.set_conw_r(g.conw_r)
+    lines = open(path).read().split("\n")
+    par = [float(lines[k].split()[0]) for k in (6, 7, 8)]
+    cl = float(lines[9].split()[0])
+    a = initial_parameters(g, g.freq_start, 1)
+    a[g.ncoef + 3:g.ncoef + 6] = par
+    a[g.ncoef + 6] = np.log(cl)
+    a[g.ncoef + 7] = 1.0
+    v = np.random.default_rng(0).standard_normal(g.mfit)
+    n = 3 if args.profile else 20
+    for _ in range(3):
+        g.gn_product(a, v)
+    torch.cuda.synchronize()
+    launches0 = ps.load_library().ps_kernel_launches()
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        for _ in range(args.steps * n):
+            out = g.gn_product(a, v)
+        dt = time.perf_counter() - t0
+    launches = ps.load_library().ps_kernel_launches() - launches0
+    assert np.all(np.isfinite(out))
+    N, F, C = g.n_points, g.numfac, g.ncoef
+    flop = 4.0 * N * F * C
+    rate = args.steps * n / dt
+    fp64_peak = ps.fp64_tensor_peak(local)
+    line = {"metric": "matrix-free Gauss-Newton products/sec on 1 B200", "value": rate, "unit": "products/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": 3, "ms_per_step": 1000 * dt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": (WORKLOAD_C5 if args.config == "c5" else WORKLOAD), "form": "adjoint (ps_gn_product)",
+                       "products_per_step": n},
+            "roofline": {"bound": "tensor", "achieved": flop * rate / 1e12, "peak": fp64_peak, "unit": "TFLOP/s",
+                         "frac": flop * rate / 1e12 / fp64_peak, "flop_rule": "4 N F C per product",
+                         "peak_source": "FP64 tensor-core throughput measured live on this GPU"},
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "e2e": {"value": rate, "unit": "products/s", "h2d_bytes_per_step": int(n * 8 * (g.ma + g.ma)),
+                    "d2h_bytes_per_step": int(n * 8 * (g.mfit + 1))}}
+    g.close()
     print(json.dumps(line), flush=True)
 
 
@@ -397,7 +472,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--periods-per-step", type=int, default=592)
-    ap.add_argument("--form", default="fast", choices=["fp64", "fast", "mixed"],
+    ap.add_argument("--form", default="fast", choices=["fp64", "fast", "mixed", "adjoint"],
                     help="fast: FP64 with the shape block on FP64 tensor cores (the headline); fp64: reference operation order")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -431,6 +506,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, path, rank)
+        return
+    if args.form == "adjoint":
+        run_adjoint(args, path, local)
         return
 
     import numpy as np

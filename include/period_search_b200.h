@@ -27,7 +27,13 @@ enum {
     PS_ERR_CUDA = 3,        /* CUDA runtime failure (message in ps_last_error) */
     PS_ERR_SINGULAR = 4,    /* singular ellipsoid-fit matrix (ludcmp) */
     PS_ERR_ARG = 5,         /* invalid argument */
-    PS_ERR_DEVICE_LOOP = 6  /* a device loop hit its iteration guard */
+    PS_ERR_DEVICE_LOOP = 6  /* a device loop hit its iteration guard: a bounded wait
+                               of the tensor-core pipeline (PS_FORM_MIXED) gave up;
+                               the fits it ended carry status -1 and the context
+                               stays usable.  The environment variable
+                               PS_B200_MAX_POLLS, read when a context opens,
+                               sets that wait limit in polls (default 2^24; 0 makes
+                               every such wait give up at once) */
 };
 
 /* Numerical form of the fit kernels. */
@@ -173,8 +179,11 @@ int ps_batch_scan(ps_batch* batch, const int* n_from, const int* n_to, ps_record
 /* Same into device memory, launched on `stream` (NULL = the batch's own
  * stream); asynchronous. */
 int ps_batch_scan_device(ps_batch* batch, const int* n_from, const int* n_to, ps_record* d_out, void* stream);
-/* SM clock cycles spent on each asteroid's fits in the last scan. */
-int ps_batch_fit_cycles(ps_batch* batch, long long* cycles);
+/* Per asteroid of the last scan: busy_ms, the time its fits ran (summed
+ * over its fits, each on its own CTA), and done_ms, the wall time from the
+ * start of the scan's first fit to the end of the asteroid's last fit (its
+ * latency inside the batch); from the GPU's global timer. */
+int ps_batch_fit_times(ps_batch* batch, double* busy_ms, double* done_ms);
 void ps_batch_close(ps_batch* batch);
 
 /* One LM fit at trial frequency freq [1/day] from initial pole m (1..10)

@@ -30,6 +30,7 @@ __all__ = [
     "start",
     "unprepare",
     "format_record",
+    "open_many",
 ]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -114,7 +115,7 @@ EXPORTS = (
     "ps_open_file", "ps_open", "ps_close", "ps_precalc", "ps_set_conw_r", "ps_n_periods", "ps_scan",
     "ps_scan_device", "ps_fit", "ps_mrqcof", "ps_model", "ps_info", "ps_get_array", "ps_open_host_only",
     "ps_format_record", "ps_last_error", "ps_kernel_launches", "ps_scan_device_noalloc",
-    "ps_batch_open", "ps_batch_scan", "ps_batch_scan_device", "ps_batch_fit_cycles", "ps_batch_close",
+    "ps_batch_open", "ps_batch_scan", "ps_batch_scan_device", "ps_batch_fit_times", "ps_batch_close",
     "ps_fp64_tensor_peak", "ps_chi2_grad", "ps_gn_product", "ps_set_tiles", "ps_autotune",
     "ps_release_cached_memory",
 )
@@ -151,7 +152,7 @@ def load_library(path: str | None = None):
         "ps_batch_open": (ctypes.c_int, [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]),
         "ps_batch_scan": (ctypes.c_int, [vp, _I, _I, vp]),
         "ps_batch_scan_device": (ctypes.c_int, [vp, _I, _I, vp, vp]),
-        "ps_batch_fit_cycles": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_longlong)]),
+        "ps_batch_fit_times": (ctypes.c_int, [vp, _D, _D]),
         "ps_batch_close": (None, [vp]),
         "ps_kernel_launches": (ctypes.c_longlong, []),
         "ps_fp64_tensor_peak": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
@@ -337,10 +338,14 @@ class PeriodSearchBatch:
         _check(self._lib.ps_batch_scan_device(self._h, a.ctypes.data_as(_I), b.ctypes.data_as(_I),
                                               ctypes.c_void_p(d_out_ptr), ctypes.c_void_p(stream_ptr or None)))
 
-    def fit_cycles(self) -> np.ndarray:
-        c = np.zeros(len(self._ctx), dtype=np.int64)
-        _check(self._lib.ps_batch_fit_cycles(self._h, c.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
-        return c
+    def fit_times(self):
+        """(busy_ms, done_ms) per asteroid of the last scan: summed fit time,
+        and wall time from the scan's first fit start to the asteroid's last
+        fit end."""
+        busy = np.zeros(len(self._ctx))
+        done = np.zeros(len(self._ctx))
+        _check(self._lib.ps_batch_fit_times(self._h, _dptr(busy), _dptr(done)))
+        return busy, done
 
     @staticmethod
     def autotune(contexts, n_from, n_to, n_periods: int = 60):
@@ -412,6 +417,34 @@ def _make_desc(d: dict):
     s.ia_par = (ctypes.c_int * 3)(*d["ia_par"])
     keep["_struct"] = s
     return keep, s
+
+
+def open_many(paths, *, device: int = 0, form: int = PS_FORM_FP64, conw_r=None, threads: int | None = None):
+    """Open one context per input file concurrently (for a batch): each
+    asteroid's host setup -- parsing, the ellipsoid fit, the facet and
+    spherical-harmonic tables (period_search_BOINC.cpp:277-485, sphfunc.c,
+    ellfit.c) -- and its uploads run on a pool of host threads (the C calls
+    release the GIL; facet-grid tables shared by asteroids with the same
+    nrows/lmax/mmax are built once).  conw_r: None leaves it unset, "start"
+    uses each asteroid's pre-pass start value conw/escl^2, a number sets it.
+    Returns the contexts in the order of `paths`."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    paths = list(paths)
+
+    def one(p):
+        c = PeriodSearch(p, device=device, form=form)
+        if conw_r == "start":
+            c.set_conw_r(c.conw_r)
+        elif conw_r is not None:
+            c.set_conw_r(float(conw_r))
+        return c
+
+    n = threads or min(len(paths), os.cpu_count() or 1, 32)
+    if n <= 1:
+        return [one(p) for p in paths]
+    with ThreadPoolExecutor(n) as ex:
+        return list(ex.map(one, paths))
 
 
 def fp64_tensor_peak(device: int = 0) -> float:

@@ -9,6 +9,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -153,6 +154,13 @@ int upload_mixed(ps_ctx* c) {
     c->dp.bsw = c->d_bsw.p;
     c->dp.nchunk = nchunk;
     c->dp.err = c->d_err.p;
+    // PS_B200_MAX_POLLS lowers the wait limit (a test makes the waits give up
+    // this way); the default is far above any wait a healthy GPU needs
+    c->dp.max_polls = 1u << 24;
+    if (const char* v = std::getenv("PS_B200_MAX_POLLS")) {
+        const long n = std::strtol(v, nullptr, 10);
+        if (n >= 0 && n <= (1l << 30)) c->dp.max_polls = (unsigned int)n;  // 0: give up at once
+    }
     return PS_OK;
 }
 
@@ -161,7 +169,12 @@ int check_device_error(ps_ctx* c) {
     if (c->form != PS_FORM_MIXED || !c->d_err.p) return PS_OK;
     int e = 0;
     PSB_CUDA(cudaMemcpy(&e, c->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
-    if (e) return fail(PS_ERR_DEVICE_LOOP, "a device wait on the tensor-core pipeline gave up (" + std::to_string(e) + ")");
+    if (e) {
+        // reported once; the context stays usable
+        PSB_CUDA(cudaMemset(c->d_err.p, 0, sizeof(int)));
+        return fail(PS_ERR_DEVICE_LOOP, "a device wait on the tensor-core pipeline gave up (" + std::to_string(e) +
+                                            "); the fits it ended carry status -1");
+    }
     return PS_OK;
 }
 

@@ -269,8 +269,8 @@ int ps_batch_scan(ps_batch* b, const int* n_from, const int* n_to, ps_record* ou
     return PS_OK;
 }
 
-int ps_batch_fit_cycles(ps_batch* b, long long* cycles) {
-    if (!b || !cycles) return psb::set_error(PS_ERR_ARG, "null argument");
+int ps_batch_fit_times(ps_batch* b, double* busy_ms, double* done_ms) {
+    if (!b || !busy_ms || !done_ms) return psb::set_error(PS_ERR_ARG, "null argument");
     PSB_BCUDA(cudaSetDevice(b->device));
     PSB_BCUDA(cudaStreamSynchronize(b->stream));
     if (b->last) PSB_BCUDA(cudaStreamSynchronize(b->last));
@@ -278,10 +278,22 @@ int ps_batch_fit_cycles(ps_batch* b, long long* cycles) {
     const size_t fits = (size_t)b->h_ctl[0];
     std::vector<psb::FitOut> f(fits);
     PSB_BCUDA(cudaMemcpy(f.data(), b->d_fits.p, fits * sizeof(psb::FitOut), cudaMemcpyDeviceToHost));
+    // times relative to the first fit's end (32-bit microsecond stamps wrap
+    // after 71 minutes; differences within a scan are well inside that)
+    const unsigned int ref = fits ? f[0].end_us : 0;
+    long long t0 = 0;  // the scan's first fit start
+    for (size_t w = 0; w < fits; w++) {
+        const long long start = (long long)(int)(f[w].end_us - ref) - (long long)f[w].dur_us;
+        if (w == 0 || start < t0) t0 = start;
+    }
     for (int a = 0; a < n; a++) {
-        long long s = 0;
-        for (int w = b->h_ctl[ctl_fit_off(n) + a]; w < b->h_ctl[ctl_fit_off(n) + a + 1]; w++) s += f[(size_t)w].cycles;
-        cycles[a] = s;
+        long long busy = 0, done = 0;
+        for (int w = b->h_ctl[ctl_fit_off(n) + a]; w < b->h_ctl[ctl_fit_off(n) + a + 1]; w++) {
+            busy += f[(size_t)w].dur_us;
+            done = std::max(done, (long long)(int)(f[(size_t)w].end_us - ref) - t0);
+        }
+        busy_ms[a] = busy * 1e-3;
+        done_ms[a] = done * 1e-3;
     }
     return PS_OK;
 }

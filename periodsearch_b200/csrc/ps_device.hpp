@@ -36,6 +36,7 @@ struct DevProblem {
     const uint16_t* bsw;         // [nchunk][2][64 x 64] BF16 hi/lo of Dsph, swizzled K-major tiles
     int nchunk;                  // facet chunks of 64 (F padded up)
     int* err;                    // device error word (bounded waits that gave up)
+    unsigned int max_polls;      // polls of an ordinary bounded wait before it gives up
     // scalars
     double phi0, conw_r, alamda_start, alamda_incr, log_cl, par1, par2, par3, ndata_m3;
     double freq_start, freq_step;
@@ -47,7 +48,8 @@ struct DevProblem {
 struct FitOut {
     double dev, dark, totarea, prd, la, be, chisq;
     int niter, status;
-    long long cycles;  // SM clock cycles the fit took (per-asteroid timing)
+    unsigned int dur_us;  // the fit's duration [us] by the GPU's global timer
+    unsigned int end_us;  // the global timer at the fit's end [us], low 32 bits
 };
 static_assert(sizeof(FitOut) == 72, "the C ABI documents 72 bytes per fit");
 

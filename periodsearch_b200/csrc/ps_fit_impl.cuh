@@ -23,6 +23,7 @@ using namespace fitcommon;
 
 constexpr int kFch = 32;     // facets per shared-memory chunk (reference-order form)
 constexpr int kRt = 32;      // rows per alpha tile (reference-order form)
+constexpr int kMf = 128;     // facets per staged chunk of the model-only pass
 // The fast form takes its facet-chunk and alpha row-tile sizes and both forms
 // the point-sort segment from the problem (DevProblem::fch, rt, sortseg):
 // runtime tile shapes, chosen by ps_autotune; no choice changes any result.
@@ -75,6 +76,7 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     int w = chunk > tile ? chunk : tile;
     if (P.mfit + 2 > w) w = P.mfit + 2;
     if (P.sortseg > w) w = P.sortseg;  // sort keys (uint64) before the point loop
+    if (3 * kMf > w) w = 3 * kMf;      // model-only pass: staged facet normals
     if (gj_buf_doubles(P.mfit) > w) w = gj_buf_doubles(P.mfit);  // Gauss-Jordan buffers
     PSB_TAKE(perm, P.sortseg / 2)
     PSB_TAKE(work, w)
@@ -178,6 +180,13 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
+}
+
+// The GPU's global nanosecond timer (the same clock on every SM).
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
 }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
@@ -562,27 +571,9 @@ __device__ __forceinline__ void alpha_tensor(const DevProblem& P, const double* 
 // dynamic shared-memory base declared here, not as pointers: a pointer
 // argument of this out-of-line function would be a generic address, and every
 // access through it a generic load or store instead of a shared-memory one.
-template <int NCB, bool kFast>
-__device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_off, int alpha_off, int beta_off,
-                                      double* Jt, double* yt) {
-    extern __shared__ __align__(16) double sm[];
-    const double* a = sm + a_off;
-    double* alpha_out = sm + alpha_off;
-    double* beta_out = sm + beta_off;
-    const DevProblem& P = *Pp;
-    const Layout L = make_layout(P);
-    const int tid = threadIdx.x;
-    const int F = P.F, C = P.C, ma = P.ma, npad = P.npad, mfit = P.mfit;
-    double* g = sm + L.g;
-    double* area = sm + L.area;
-    double* misc = sm + L.misc;
-    double* B = sm + L.blm;
-    double* D = sm + L.blm + 9;
-    double* dres = sm + L.dres;
-    double* work = sm + L.work;
-
-    // blmatrix (mrqcof.c:34) and the per-evaluation scalars of bright.c:26-33
-    if (tid == 0) {
+// blmatrix (mrqcof.c:34) and the per-evaluation scalars of bright.c:26-33.
+__device__ __forceinline__ void eval_scalars(const double* a, int C, double* B, double* D, double* misc) {
+    if (threadIdx.x == 0) {
         blmatrix(a[C], a[C + 1], B, D);
         misc[M_CL] = exp(a[C + 6]);
         misc[M_CLS] = a[C + 7];
@@ -591,8 +582,13 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_o
         misc[M_P2] = a[C + 4];
         misc[M_P3] = a[C + 5];
     }
-    // curv.c:15-37: g = exp(sum over (m, l) of Pleg * (c*Fc + s*Fs))
-    for (int f = tid; f < F; f += kThreads) {
+}
+
+// curv.c:15-37: g = exp(sum over (m, l) of Pleg * (c*Fc + s*Fs)), thread per
+// facet; area = Darea g, zero for the 128 slots past F.
+__device__ __forceinline__ void curv_phase(const DevProblem& P, const double* a, double* g, double* area) {
+    const int F = P.F;
+    for (int f = threadIdx.x; f < F; f += kThreads) {
         const double* pl = P.cpl + (size_t)f * P.nq;
         const double* fc = P.cfc + (size_t)f * (P.mmax + 1);
         const double* fs = P.cfs + (size_t)f * (P.mmax + 1);
@@ -615,7 +611,174 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_o
         g[f] = gi;
         area[f] = P.fac[(size_t)f * 4 + 3] * gi;
     }
-    for (int f = F + tid; f < F + 128; f += kThreads) area[f] = 0.0;
+    for (int f = F + threadIdx.x; f < F + 128; f += kThreads) area[f] = 0.0;
+}
+
+// chi2 over all rows (mrqcof.c:119-135) from the normalised model yt.  The
+// reference-order form sums the rows in order on one thread, with the
+// operations of its alpha/beta/chi2 phase (whose chi2 entry is the same
+// sum), so both give the same bits; the fast form sums on one warp in a
+// fixed order.  The result lands in misc[M_CHISQ].
+template <bool kFast>
+__device__ __forceinline__ void chi2_rows(const DevProblem& P, const double* yt, double* misc) {
+    if constexpr (!kFast) {
+        if (threadIdx.x == 0) {
+            double acc = 0;
+            for (int r = 0; r < P.n_rows; r++) {
+                const double dy = P.yobs[r] - yt[r];
+                acc = acc + dy * dy * P.sig2i[r] * P.wght[r];
+            }
+            misc[M_CHISQ] = acc;
+        }
+    } else {
+        if (threadIdx.x < 32) {
+            double acc = 0;
+            for (int r = threadIdx.x; r < P.n_rows; r += 32) {
+                const double dy = P.yobs[r] - yt[r];
+                acc = fma(dy * P.sig2i[r] * P.wght[r], dy, acc);
+            }
+#pragma unroll
+            for (int o = 16; o >= 1; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+            if (threadIdx.x == 0) misc[M_CHISQ] = acc;
+        }
+    }
+}
+
+// The model alone at parameters a (sm offset a_off): what the LM step's
+// accept/reject test and the stop rule read from mrqcof at a trial point --
+// chi2, the convexity residuals chck (conv.c:22-27) and the facet-area sum --
+// without the Jacobian or alpha/beta.  curv, the brightness of every point
+// (bright.c:54-76, 106-125 without the derivative terms), the convexity
+// rows, the relative-lightcurve normalisation of the model (mrqcof.c:53-58,
+// 92-104) and chi2, with the operations and sum orders of evaluate(), so
+// that in the reference-order form every value is bit-identical to the one
+// evaluate() gives at the same point.  The model goes to yt; Jt is not
+// touched.  Thread per data point, facet normals staged in chunks of kMf.
+template <int NCB, bool kFast>
+__device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, int a_off, double* yt) {
+    extern __shared__ __align__(16) double sm[];
+    const double* a = sm + a_off;
+    const DevProblem& P = *Pp;
+    const Layout L = make_layout(P);
+    const int tid = threadIdx.x;
+    const int F = P.F, C = P.C;
+    double* g = sm + L.g;
+    double* area = sm + L.area;
+    double* misc = sm + L.misc;
+    double* B = sm + L.blm;
+    double* D = sm + L.blm + 9;
+    double* work = sm + L.work;
+    eval_scalars(a, C, B, D, misc);
+    curv_phase(P, a, g, area);
+    __syncthreads();
+    // chck and the facet-area sum, facets in order (as evaluate() and the
+    // fast point loop form them)
+    if (tid < 4) {
+        double s = 0;
+        if (tid < 3) {
+            for (int f = 0; f < F; f++) s = s + area[f] * P.fac[(size_t)f * 4 + tid];
+            misc[M_CHK0 + tid] = s;
+        } else {
+            for (int f = 0; f < F; f++) s = s + area[f];
+            misc[M_SAREA] = s;
+        }
+    }
+    const double cl = misc[M_CL], cls = misc[M_CLS];
+    for (int base = 0; base < P.n_points; base += kThreads) {
+        const int p = base + tid;
+        const bool act = p < P.n_points;
+        double e0_ = 0, e1_ = 0, e2_ = 0, f0_ = 0, f1_ = 0, f2_ = 0, sc = 0;
+        if (act) {
+            PointGeom G;
+            point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
+            e0_ = G.e[0];
+            e1_ = G.e[1];
+            e2_ = G.e[2];
+            f0_ = G.e0[0];
+            f1_ = G.e0[1];
+            f2_ = G.e0[2];
+            sc = G.scale;
+        }
+        double br = 0;
+        for (int c0 = 0; c0 < F; c0 += kMf) {
+            const int nf = min(kMf, F - c0);
+            __syncthreads();
+            for (int i = tid; i < nf * 3; i += kThreads) {
+                const int ff = i / 3, k = i - ff * 3;
+                work[i] = P.fac[(size_t)(c0 + ff) * 4 + k];
+            }
+            __syncthreads();
+            if (act) {
+#pragma unroll 4
+                for (int ff = 0; ff < nf; ff++) {
+                    const double nx = work[ff * 3 + 0], ny = work[ff * 3 + 1], nz = work[ff * 3 + 2];
+                    const double mu = e0_ * nx + e1_ * ny + e2_ * nz;
+                    const double mu0 = f0_ * nx + f1_ * ny + f2_ * nz;
+                    if ((mu > kTinyD) && (mu0 > kTinyD)) {
+                        const double ar = area[c0 + ff];
+                        if constexpr (kFast) {
+                            const double r = 1.0 / (mu + mu0);
+                            br = fma(ar, mu * mu0 * fma(cls, r, cl), br);
+                        } else {
+                            const double dnom = mu + mu0;
+                            const double s = mu * mu0 * (cl + cls / dnom);
+                            br = br + ar * s;
+                        }
+                    }
+                }
+            }
+        }
+        if (act) yt[p] = br * sc;
+    }
+    __syncthreads();
+    if (tid < 3) yt[P.n_points + tid] = misc[M_CHK0 + tid];
+    // relative-lightcurve normalisation of the model, mrqcof.c:53-58, 92-104
+    for (int lc0 = 0; lc0 < P.n_lc; lc0 += kThreads) {
+        __syncthreads();
+        const int lc = lc0 + tid;
+        if (lc < P.n_lc && P.lc_rel[lc]) {
+            double s = 0;
+            for (int r = P.lc_start[lc]; r < P.lc_start[lc + 1]; r++) s = s + yt[r];
+            work[tid] = s;
+        }
+        __syncthreads();
+        for (int k = 0; k < kThreads && lc0 + k < P.n_lc; k++) {
+            const int l2 = lc0 + k;
+            if (!P.lc_rel[l2]) continue;
+            const double ave = work[k];
+            const double lpts = (double)P.lc_npts[l2];
+            for (int r = P.lc_start[l2] + tid; r < P.lc_start[l2 + 1]; r += kThreads) {
+                const double coef = P.sig[r] * lpts / ave;
+                yt[r] = coef * yt[r];
+            }
+        }
+    }
+    __syncthreads();
+    chi2_rows<kFast>(P, yt, misc);
+    __syncthreads();
+}
+
+template <int NCB, bool kFast>
+__device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_off, int alpha_off, int beta_off,
+                                      double* Jt, double* yt) {
+    extern __shared__ __align__(16) double sm[];
+    const double* a = sm + a_off;
+    double* alpha_out = sm + alpha_off;
+    double* beta_out = sm + beta_off;
+    const DevProblem& P = *Pp;
+    const Layout L = make_layout(P);
+    const int tid = threadIdx.x;
+    const int F = P.F, C = P.C, ma = P.ma, npad = P.npad, mfit = P.mfit;
+    double* g = sm + L.g;
+    double* area = sm + L.area;
+    double* misc = sm + L.misc;
+    double* B = sm + L.blm;
+    double* D = sm + L.blm + 9;
+    double* dres = sm + L.dres;
+    double* work = sm + L.work;
+
+    eval_scalars(a, C, B, D, misc);
+    curv_phase(P, a, g, area);
     __syncthreads();
     // Sequential facet sums: chck / conv residuals (conv.c:22-27), the
     // facet-area sum (period_search_BOINC.cpp:900-902) and the conv-row shape
@@ -826,6 +989,10 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_o
     }
     if constexpr (kFast) {
         alpha_tensor<NCB>(P, Jt, yt, work, alpha_out, beta_out, misc);
+        // chi2 as the model-only pass sums it, so that the LM test compares
+        // values of one rounding
+        __syncthreads();
+        chi2_rows<true>(P, yt, misc);
     } else {
         // alpha = J^T W J, beta = J^T W dy, chi2 (mrqcof.c:106-147), every entry
         // summing the rows in order.  Tile of kRt rows: Ws[r][j] = (J[r][l_j]
@@ -970,7 +1137,7 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
             cur_mfit = mfit;
             cur_ent = L.ent;
         }
-        const long long t_start = clock64();
+        const unsigned long long t_start = global_ns();
         double freq;
         int pole;
         if (Bt.pole_override) {
@@ -1010,6 +1177,16 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
         // Levenberg-Marquardt loop, period_search_BOINC.cpp:846-893, with
         // mrqmin (mrqmin.c:11-110) inlined.  Scalars are kept identically in
         // every thread.
+        //
+        // mrqmin evaluates mrqcof in full at every trial point, but alpha and
+        // beta from a trial point are only used when the step is accepted
+        // (mrqmin.c:91-101); about half the steps of these fits are rejected.
+        // So a trial point gets the model alone (evaluate_model: chi2, chck,
+        // facet-area sum -- all the accept/reject test and the stop rule
+        // read), and the Jacobian with alpha and beta is evaluated at the new
+        // point only when the next step needs it (j_stale), which also skips
+        // it after the last step.  Every value, and so every result, is the
+        // same as with a full evaluation per step.
         double* alpha = sm + L.alpha;
         double* covar = sm + L.covar;
         double* beta = sm + L.beta;
@@ -1017,6 +1194,7 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
         double alamda = -1, ochisq = 0, chisq = 0, iter_diff = 1e40, dev_old = 1e30, dev_new = 0, rchisq = -1;
         double chk0 = 0, chk1 = 0, chk2 = 0, cur0 = 0, cur1 = 0, cur2 = 0, s_cur = 0, s_last = 0;
         int niter = 0, status = 0;
+        bool j_stale = false;
         while (((niter < P.n_iter_max) && (iter_diff > P.iter_diff_max)) || (niter < P.n_iter_min)) {
             if (alamda < 0) {
                 alamda = P.alamda_start;
@@ -1027,6 +1205,11 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
                 cur2 = misc[M_CHK0 + 2];
                 s_cur = s_last = misc[M_SAREA];
                 for (int i = tid; i < ma; i += kThreads) atry[i] = cg[i];
+            } else if (j_stale) {
+                // alpha and beta at the point accepted last (its chi2, chck and
+                // area sum came from the model-only evaluation and are kept)
+                evaluate<NCB, kFast>(Pp, (int)(cg - sm), (int)(alpha - sm), (int)(beta - sm), Jt, yt);
+                j_stale = false;
             }
             for (int idx = tid; idx < mfit * mfit; idx += kThreads) {
                 const int j = idx / mfit, k = idx - j * mfit;
@@ -1042,20 +1225,13 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
                     atry[l] = cg[l] + da[j];
                 }
                 __syncthreads();
-                // alpha/covar and beta/da trade places on every accepted step: the
-                // offsets follow the pointers
-                evaluate<NCB, kFast>(Pp, (int)(atry - sm), (int)(covar - sm), (int)(da - sm), Jt, yt);
+                evaluate_model<NCB, kFast>(Pp, (int)(atry - sm), yt);
                 const double temp = misc[M_CHISQ];
                 chisq = temp;
                 s_last = misc[M_SAREA];
                 if (temp < ochisq) {
                     alamda = alamda / P.alamda_incr;
-                    double* t1 = alpha;
-                    alpha = covar;
-                    covar = t1;
-                    t1 = beta;
-                    beta = da;
-                    da = t1;
+                    j_stale = true;
                     for (int i = tid; i < ma; i += kThreads) cg[i] = atry[i];
                     cur0 = misc[M_CHK0];
                     cur1 = misc[M_CHK0 + 1];
@@ -1099,7 +1275,9 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
             o.chisq = chisq;
             o.niter = niter;
             o.status = status;
-            o.cycles = clock64() - t_start;
+            const unsigned long long t_end = global_ns();
+            o.dur_us = (unsigned int)((t_end - t_start) / 1000ull);
+            o.end_us = (unsigned int)(t_end / 1000ull);
             Bt.out[w] = o;
         }
     }

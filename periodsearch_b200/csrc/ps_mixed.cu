@@ -47,7 +47,12 @@ constexpr int kKc = 64;         // facets per chunk (one swizzled 128-byte row)
 constexpr int kNc = 64;         // MMA N (shape coefficients, C <= 64)
 constexpr int kRtM = 32;        // rows per alpha tile
 constexpr int kMaxEptM = 16;    // alpha/beta/chi2 entries per thread
-constexpr uint32_t kMaxPolls = 1u << 24;
+// Bounded waits: the ordinary waits on the tensor core take P.max_polls
+// polls at most (ps_open sets it, by default kMaxPolls); a wait that gives up
+// ends the fit: the CTA stops taking work, waits for its own MMAs in flight
+// with the fixed kDrainPolls limit, frees its TMEM and returns, and the host
+// reports PS_ERR_DEVICE_LOOP.
+constexpr uint32_t kDrainPolls = 1u << 26;
 constexpr uint32_t kTmemCols = 64;
 
 // Shared memory: a 1024-byte aligned block of MMA operand tiles followed by
@@ -135,7 +140,8 @@ enum {
     M_P1 = 8,
     M_P2 = 9,
     M_P3 = 10,
-    M_WORK = 11
+    M_WORK = 11,
+    M_ABORT = 12  // a bounded wait of the last evaluation gave up
 };
 
 struct MPtr {
@@ -181,7 +187,7 @@ __device__ __noinline__ void evaluate_mixed(const DevProblem* __restrict__ Pp, u
     uint64_t* mbar = (uint64_t*)(M.base + L.mbar);
     const int* ent = M.ints + L.ent;
     uint32_t gc = *gc_io;
-    bool wait_ok = true;
+    bool aborted = false;
 
     if (tid == 0) {
         blmatrix(a[C], a[C + 1], B, D);
@@ -250,7 +256,13 @@ __device__ __noinline__ void evaluate_mixed(const DevProblem* __restrict__ Pp, u
         float T0 = 0, T1 = 0, T2 = 0, S0 = 0, S1 = 0, S2 = 0, scl = 0, scls = 0;
         for (int ch = 0; ch < nch; ch++, gc++) {
             const int buf = gc & 1;
-            if (gc >= 2 && !umma::mbar_wait(&mbar[buf], ((gc - 2) >> 1) & 1, kMaxPolls)) wait_ok = false;
+            // operand buffer `buf` is free once the MMAs of chunk gc - 2 are done
+            bool fail = false;
+            if (tid == 0 && gc >= 2) fail = !umma::mbar_wait(&mbar[buf], ((gc - 2) >> 1) & 1, P.max_polls);
+            if (__syncthreads_or(fail)) {
+                aborted = true;
+                break;
+            }
             // Y chunk (hi, lo) into the B tiles: 16 KB, 4 x 16 B per thread
             {
                 const uint4* src = (const uint4*)(P.bsw + (size_t)ch * 2 * kNc * kKc);
@@ -348,12 +360,17 @@ __device__ __noinline__ void evaluate_mixed(const DevProblem* __restrict__ Pp, u
             e[6] = scl;
             e[7] = scls;
         }
+        if (aborted) break;
         // wait for the tile's last MMA before reading the accumulator
         {
             const uint32_t last = gc - 1;
-            if (!umma::mbar_wait(&mbar[last & 1], (last >> 1) & 1, kMaxPolls)) wait_ok = false;
+            bool fail = false;
+            if (tid == 0) fail = !umma::mbar_wait(&mbar[last & 1], (last >> 1) & 1, P.max_polls);
+            if (__syncthreads_or(fail)) {
+                aborted = true;
+                break;
+            }
         }
-        __syncthreads();
         umma::fence_after_sync();
         if (half == 0) {
             // warps 0-3: TMEM lanes 32w..32w+31 hold points base + 32w + lane
@@ -403,6 +420,16 @@ __device__ __noinline__ void evaluate_mixed(const DevProblem* __restrict__ Pp, u
         __syncthreads();
     }
     __syncthreads();
+    if (aborted) {
+        if (tid == 0) {
+            atomicAdd(P.err, 1);
+            misc[M_CHISQ] = __longlong_as_double(0x7ff8000000000000ll);
+            misc[M_ABORT] = 1;
+        }
+        *gc_io = gc;
+        __syncthreads();
+        return;
+    }
     // convexity rows
     for (int job = tid; job < 3 * ma; job += kThreads) {
         const int nc = job / ma, l = job - nc * ma;
@@ -510,7 +537,6 @@ __device__ __noinline__ void evaluate_mixed(const DevProblem* __restrict__ Pp, u
             }
         }
     }
-    if (!wait_ok) atomicAdd(P.err, 1);
     *gc_io = gc;
     __syncthreads();
 }
@@ -523,6 +549,7 @@ __device__ void tmem_setup(const DevProblem& P, uint8_t* raw, uint32_t* tmem) {
     if (threadIdx.x == 0) {
         umma::mbar_init(&mbar[0], 1);
         umma::mbar_init(&mbar[1], 1);
+        umma::mbar_init(&mbar[2], 1);  // the final drain
     }
     umma::fence_before_sync();
     __syncthreads();
@@ -530,7 +557,15 @@ __device__ void tmem_setup(const DevProblem& P, uint8_t* raw, uint32_t* tmem) {
     *tmem = *slot;
 }
 
-__device__ void tmem_teardown(uint32_t tmem) {
+// Every MMA this CTA issued completes (bounded by the fixed drain limit,
+// which no setting lowers) before its TMEM is freed.
+__device__ void tmem_teardown(const DevProblem& P, uint8_t* raw, uint32_t tmem) {
+    const MPtr M = mptrs(P, raw);
+    uint64_t* mbar = (uint64_t*)(M.base + M.L.mbar);
+    if (threadIdx.x == 0) {
+        umma::commit(&mbar[2]);
+        if (!umma::mbar_wait(&mbar[2], 0, kDrainPolls)) atomicAdd(P.err, 1);
+    }
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
@@ -554,8 +589,10 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
     uint32_t gc = 0;
     float* Jf = (float*)(Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride);
     double* yt = Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride + ((size_t)ma * P.npad + 1) / 2;
+    if (tid == 0) misc[M_ABORT] = 0;
+    bool aborted = false;
 
-    for (;;) {
+    while (!aborted) {
         __syncthreads();
         if (tid == 0) misc[M_WORK] = (double)atomicAdd(Bt.queue, 1);
         __syncthreads();
@@ -606,6 +643,10 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
             if (alamda < 0) {
                 alamda = P.alamda_start;
                 evaluate_mixed(Pp, smem_raw, cg, alpha, beta, Jf, yt, tmem, &gc);
+                if (misc[M_ABORT] != 0) {
+                    aborted = true;
+                    break;
+                }
                 ochisq = misc[M_CHISQ];
                 cur0 = misc[M_CHK0];
                 cur1 = misc[M_CHK0 + 1];
@@ -628,6 +669,10 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
                 }
                 __syncthreads();
                 evaluate_mixed(Pp, smem_raw, atry, covar, da, Jf, yt, tmem, &gc);
+                if (misc[M_ABORT] != 0) {
+                    aborted = true;
+                    break;
+                }
                 const double temp = misc[M_CHISQ];
                 chisq = temp;
                 s_last = misc[M_SAREA];
@@ -676,14 +721,15 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
             o.prd = 2 * kPiD / cg[C + 2];
             o.la = (180 / kPiD) * cg[C + 1];
             o.be = 90 - (180 / kPiD) * cg[C];
-            o.chisq = chisq;
+            o.chisq = aborted ? __longlong_as_double(0x7ff8000000000000ll) : chisq;
             o.niter = niter;
-            o.status = status;
-            o.cycles = 0;
+            o.status = aborted ? -1 : status;
+            o.dur_us = 0;
+            o.end_us = 0;
             Bt.out[w] = o;
         }
     }
-    tmem_teardown(tmem);
+    tmem_teardown(P, smem_raw, tmem);
 }
 
 __global__ void __launch_bounds__(kThreads, 1) mixed_eval_kernel(const DevProblem* __restrict__ Pp, EvalOut E) {
@@ -710,7 +756,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_eval_kernel(const DevProble
         E.J[idx] = (double)Jf[(size_t)l * P.npad + r];
     }
     for (int r = tid; r < P.n_rows; r += kThreads) E.y[r] = yt[r];
-    tmem_teardown(tmem);
+    tmem_teardown(P, smem_raw, tmem);
 }
 
 bool mixed_supported(const DevProblem& P) {

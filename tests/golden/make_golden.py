@@ -33,6 +33,16 @@ Inputs:
   unit      golden arrays of the reference's unit tests
             (period_search_pure_cpu_win/UnitTest_pure_cpu_win/arrangers.cpp),
             dumped to unit.json through a small C++ harness
+  c2        the benchmarked production size: 20 trial periods spread over
+            2-100 h, from the reference application (+ FMA build, variants)
+  c4_shaped three large asteroids of the uneven batch (up to 4 793 points,
+            convergence rule) and c5 (one period of the 20 000-point,
+            2 048-facet workload): beyond the reference application's static
+            arrays, so from the restatement (-O3, fma, sq builds); their
+            inputs are regenerated by periodsearch_b200.synth at test time
+            and checked against the sha256 stored in meta.json
+
+Not in the default set (minutes of CPU each): c2, c4_shaped, c5.
 """
 from __future__ import annotations
 
@@ -239,6 +249,150 @@ def make_unit():
         shutil.rmtree(d, ignore_errors=True)
 
 
+C2_PERIODS = 20  # trial periods of the c2 slice, spread evenly over its 2-100 h range
+C4_ASTEROIDS = (7, 42, 180)  # c4 asteroids with the most points: 39 lightcurves / one 3715- / one 4581-point set
+C4_PERIODS = 2
+C5_PERIOD = 1
+
+
+def _sha(text):
+    import hashlib
+
+    return hashlib.sha256(text.encode()).hexdigest()
+
+
+def c2_text():
+    """The c2 production workload (N 760, lmax 6, nrows 10, 2-100 h) with the
+    convexity weight set to the value its pre-pass ends at (conw x 2^5): the
+    reference's pre-pass then stops after one round of 100 fits instead of
+    six, with the same conw_r (a power-of-two scaling, exact)."""
+    from periodsearch_b200 import synth
+
+    lines = synth._c2().text.split("\n")
+    assert lines[3].split()[0] == "0.1"
+    lines[3] = "3.2\t\t\t\tconvexity weight"
+    return "\n".join(lines)
+
+
+def _one_period(exe, text, n):
+    return _run_slice(exe, text, n, n)
+
+
+def make_c2_spread(workers):
+    """c2 at the benchmarked size: C2_PERIODS trial periods spread over the
+    whole 2-100 h range, each one run by the reference application itself
+    (and its FMA build) as its own slice (P_end trimmed, started through the
+    checkpoint file, pre-pass included), plus the restatement's perturbed
+    builds at the same conw_r for the chaotic-period triage."""
+    import pso
+
+    d = os.path.join(HERE, "c2")
+    os.makedirs(d, exist_ok=True)
+    text = c2_text()
+    open(os.path.join(d, "period_search_in"), "w").write(text)
+    o = pso.Oracle(os.path.join(d, "period_search_in"))
+    o.set_conw_r(o.conw_r)
+    n_total = o.n_periods
+    idx = [1 + round(k * (n_total - 1) / (C2_PERIODS - 1)) for k in range(C2_PERIODS)]
+    open(os.path.join(d, "periods.txt"), "w").write("".join("%d\n" % n for n in idx))
+    for exe, txt_name, full_name in ((REF_EXE, "ref_out.txt", "ref_out.full"), (REF_FMA, None, "fma_out.full")):
+        with cf.ProcessPoolExecutor(max_workers=workers) as ex:
+            outs = list(ex.map(_one_period, [exe] * len(idx), [text] * len(idx), idx))
+        if txt_name:
+            open(os.path.join(d, txt_name), "w").write("".join(t for t, _ in outs))
+        open(os.path.join(d, full_name), "w").write("".join(f for _, f in outs))
+        print("c2", full_name, "written", flush=True)
+    ref = pso.read_full(os.path.join(d, "ref_out.full"))
+    import math
+
+    o2 = pso.Oracle(os.path.join(d, "period_search_in"))
+    k = round(math.log2(ref["dark_pct"][0] / (o2.conw_r * o2.escl * o2.escl)))
+    conw_r = o2.conw_r * 2.0**k
+    for var in ("sq", "fma", "fmasq"):
+        exe = os.path.join(REPO, "oracle", "ps_oracle_" + var)
+        with cf.ProcessPoolExecutor(max_workers=workers) as ex:
+            outs = list(ex.map(_run_variant_slice, [exe] * len(idx), [text] * len(idx), idx, idx,
+                               [conw_r] * len(idx)))
+        open(os.path.join(d, "var_%s.full" % var), "w").write("".join(outs))
+    print("c2 variants written", flush=True)
+
+
+def _restatement_records(name, texts, n_from, n_to, conw_rs, workers):
+    """Records of the restatement (ps_oracle: -O3, its perturbed builds) for
+    inputs beyond the reference application's static arrays."""
+    d = os.path.join(HERE, name)
+    for var, exe in (("oracle_out", os.path.join(REPO, "oracle", "ps_oracle")),
+                     ("var_fma", os.path.join(REPO, "oracle", "ps_oracle_fma")),
+                     ("var_sq", os.path.join(REPO, "oracle", "ps_oracle_sq"))):
+        with cf.ProcessPoolExecutor(max_workers=workers) as ex:
+            outs = list(ex.map(_run_variant_slice, [exe] * len(texts), texts, n_from, n_to, conw_rs))
+        yield var, outs
+
+
+def make_c4_shaped(workers):
+    """Three c4 asteroids (the uneven batch's largest shapes: up to 4 793
+    points, one sparse set of 4 581 points, or 39 lightcurves; lmax 6,
+    nrows 10, the per-fit convergence rule), C4_PERIODS trial periods each at
+    the pre-pass start value conw/escl^2 as the batch benchmark runs them.
+    The reference application holds at most 1 000 points per lightcurve
+    (constants.h POINTS_MAX), so the records come from the restatement."""
+    import pso
+    from periodsearch_b200 import synth
+
+    d = os.path.join(HERE, "c4_shaped")
+    os.makedirs(d, exist_ok=True)
+    texts, conws, meta = [], [], {"asteroids": [], "periods": C4_PERIODS}
+    for i in C4_ASTEROIDS:
+        w, _ = synth.c4_asteroid(i)
+        tmp = tempfile.mkdtemp(prefix="psc4g")
+        o = pso.Oracle(synth.write_input(w, tmp))
+        texts.append(w.text)
+        conws.append(o.conw_r)
+        meta["asteroids"].append({"index": i, "sha256": _sha(w.text), "n_points": w.n_points, "conw_r": o.conw_r})
+        shutil.rmtree(tmp, ignore_errors=True)
+    for var, outs in _restatement_records("c4_shaped", texts, [1] * len(texts), [C4_PERIODS] * len(texts), conws,
+                                          workers):
+        for i, out in zip(C4_ASTEROIDS, outs):
+            open(os.path.join(d, "a%03d_%s.full" % (i, var)), "w").write(out)
+    json.dump(meta, open(os.path.join(d, "meta.json"), "w"), indent=1)
+    print("c4_shaped written", flush=True)
+
+
+def c5_workload():
+    from periodsearch_b200 import synth
+
+    return synth.make_workload("c5_lmax8_n20000_f2048", 5, dense_lcs=40, dense_pts=100, sparse_pts=16000, years=10,
+                               true_lmax=10, fit_lmax=8, nrows=16, noise=0.03, n_periods=2000)
+
+
+def make_c5(workers):
+    """One trial period (10 whole fits) of the c5 workload at full size
+    (N 20 000, lmax 8, 2 048 facets) from the restatement and its perturbed
+    builds, at the pre-pass start value conw/escl^2 (the benchmark skips the
+    pre-pass there too); 2 048 facets exceed the reference application's
+    MAX_N_FAC."""
+    import pso
+
+    d = os.path.join(HERE, "c5")
+    os.makedirs(d, exist_ok=True)
+    from periodsearch_b200 import synth
+
+    w = c5_workload()
+    tmp = tempfile.mkdtemp(prefix="psc5g")
+    o = pso.Oracle(synth.write_input(w, tmp))
+    meta = {"sha256": _sha(w.text), "conw_r": o.conw_r, "period": C5_PERIOD}
+    shutil.rmtree(tmp, ignore_errors=True)
+    jobs = []
+    for var in ("ps_oracle", "ps_oracle_fma", "ps_oracle_sq"):
+        jobs.append((os.path.join(REPO, "oracle", var), w.text, C5_PERIOD, C5_PERIOD, meta["conw_r"]))
+    with cf.ProcessPoolExecutor(max_workers=min(workers, 3)) as ex:
+        outs = list(ex.map(_run_variant_slice, *zip(*jobs)))
+    for name, out in zip(("oracle_out", "var_fma", "var_sq"), outs):
+        open(os.path.join(d, name + ".full"), "w").write(out)
+    json.dump(meta, open(os.path.join(d, "meta.json"), "w"), indent=1)
+    print("c5 written", flush=True)
+
+
 def main(names):
     from periodsearch_b200 import synth
 
@@ -274,6 +428,12 @@ def main(names):
     for name in ("tiny", "tiny_rel", "c1", "shipped", "tiny_conv", "c1_conv"):
         if name in names or "variants" in names:
             make_variants(name, workers)
+    if "c2" in names:
+        make_c2_spread(workers)
+    if "c4_shaped" in names:
+        make_c4_shaped(workers)
+    if "c5" in names:
+        make_c5(workers)
 
 
 if __name__ == "__main__":

@@ -1,0 +1,116 @@
+"""Parity at the benchmarked sizes (fixtures from tests/golden/make_golden.py).
+
+c2         the production sparse search that bench.py times (N 760, lmax 6,
+           800 facets): 20 trial periods spread over 2-100 h against the
+           reference application itself, both FP64 forms, pre-pass included;
+c4_shaped  three of the uneven batch's largest asteroids (up to 4 793 points,
+           a single 4 581-point lightcurve, 39 lightcurves; the per-fit
+           convergence rule) through the batched path;
+c5         one trial period (10 whole fits) of the 20 000-point, 2 048-facet,
+           lmax 8 workload.
+c4_shaped and c5 exceed the reference application's static arrays
+(POINTS_MAX 1 000 points per lightcurve, MAX_N_FAC 1 000 facets), so their
+records come from the restatement (pinned bit-exact to the reference on
+in-limit inputs); their inputs are regenerated by the seeded generator and
+checked against the sha256 the fixture stores.
+
+The bar is the one of test_gpu_parity.py: chi2 and rms within 1e-9, or, on a
+chaotic period (one whose chi2 the reference's own last-ulp perturbations --
+its FMA build, the restatement's x*x / FMA builds -- move by more than
+that), within ten times that spread; identical top-1/10/20 ranking."""
+import json
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, golden_path
+from test_gpu_parity import FIT_TOL, FORMS, _form, _read_full, check_records, perturbation_spread
+
+sys.path.insert(0, GOLDEN)
+import make_golden  # noqa: E402  (the fixture definitions: inputs, periods)
+
+pytestmark = pytest.mark.gpu
+
+
+def _fixture(name, *parts):
+    p = os.path.join(GOLDEN, name, *parts)
+    if not os.path.exists(p):
+        pytest.skip("fixture not generated: " + p)
+    return p
+
+
+def _spread_from(files, ref):
+    spread = np.zeros(len(ref), dtype=[("chi2", "f8"), ("lambda_deg", "f8"), ("beta_deg", "f8")])
+    for f in files:
+        if os.path.exists(f):
+            x = _read_full(f)
+            spread["chi2"] = np.maximum(spread["chi2"], np.abs(x["chi2"] - ref["chi2"]) / np.abs(ref["chi2"]))
+            for key in ("lambda_deg", "beta_deg"):
+                spread[key] = np.maximum(spread[key], np.abs(x[key] - ref[key]))
+    return spread
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_c2_spread_matches_reference(native, form):
+    ref = _read_full(_fixture("c2", "ref_out.full"))
+    idx = [int(x) for x in open(_fixture("c2", "periods.txt")).read().split()]
+    assert open(golden_path("c2")).read() == make_golden.c2_text()
+    spread = perturbation_spread("c2", ref)
+    g = native.PeriodSearch(golden_path("c2"), form=_form(native, form))
+    conw_r = g.precalc()
+    assert idx[0] == 1 and abs(conw_r * g.escl ** 2 - ref["dark_pct"][0]) <= 1e-12 * ref["dark_pct"][0]
+    recs = np.concatenate([g.scan(n, n) for n in idx])
+    n_chaotic, worst = check_records(recs, ref, spread, "c2")
+    print(f"c2 {form}: {n_chaotic} chaotic of {len(ref)} periods, worst chi2 rel err {worst:.3e}")
+    g.close()
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_c4_shaped_batch_matches_restatement(native, tmp_path, form):
+    from periodsearch_b200 import synth
+
+    meta = json.load(open(_fixture("c4_shaped", "meta.json")))
+    paths = []
+    for a in meta["asteroids"]:
+        w, _ = synth.c4_asteroid(a["index"])
+        assert make_golden._sha(w.text) == a["sha256"], "generator output changed"
+        paths.append(synth.write_input(w, str(tmp_path / ("a%03d" % a["index"]))))
+    ctxs = native.open_many(paths, form=_form(native, form))
+    for c, a in zip(ctxs, meta["asteroids"]):
+        c.set_conw_r(a["conw_r"])
+    P = meta["periods"]
+    batch = native.PeriodSearchBatch(ctxs)
+    got = batch.scan([1] * len(ctxs), [P] * len(ctxs))
+    for a, g in zip(meta["asteroids"], got):
+        base = os.path.join(GOLDEN, "c4_shaped", "a%03d_" % a["index"])
+        ref = _read_full(base + "oracle_out.full")
+        spread = _spread_from([base + "var_fma.full", base + "var_sq.full"], ref)
+        # the record's first line carries conw_r escl^2 in the restatement too
+        n_chaotic, worst = check_records(g, ref, spread, "c4_%d" % a["index"])
+        print(f"c4 asteroid {a['index']} ({a['n_points']} points) {form}: {n_chaotic} chaotic, worst {worst:.3e}")
+    batch.close()
+    for c in ctxs:
+        c.close()
+
+
+@pytest.mark.parametrize("form", FORMS)
+def test_c5_full_size_matches_restatement(native, tmp_path, form):
+    from periodsearch_b200 import synth
+
+    meta = json.load(open(_fixture("c5", "meta.json")))
+    w = make_golden.c5_workload()
+    assert make_golden._sha(w.text) == meta["sha256"], "generator output changed"
+    path = synth.write_input(w, str(tmp_path))
+    g = native.PeriodSearch(path, form=_form(native, form))
+    g.set_conw_r(meta["conw_r"])
+    n = meta["period"]
+    got = g.scan(n, n)
+    ref = _read_full(_fixture("c5", "oracle_out.full"))
+    spread = _spread_from([os.path.join(GOLDEN, "c5", "var_fma.full"), os.path.join(GOLDEN, "c5", "var_sq.full")],
+                          ref)
+    err = abs(got["chi2"][0] - ref["chi2"][0]) / ref["chi2"][0]
+    print(f"c5 {form}: chi2 rel err {err:.3e}, perturbation spread {spread['chi2'][0]:.3e}")
+    assert err <= FIT_TOL or err <= 10 * spread["chi2"][0], (err, spread["chi2"][0])
+    g.close()

@@ -95,3 +95,43 @@ def test_mixed_scan_drift(native, oracle_lib, name):
           f"max {err.max():.2e}, best period identical: {best_same}")
     assert np.median(err) <= 1e-2
     g.close()
+
+
+_WAIT_CHILD = r"""
+import sys
+sys.path.insert(0, sys.argv[1])
+import periodsearch_b200 as ps
+g = ps.PeriodSearch(sys.argv[2], form=ps.PS_FORM_MIXED)
+g.set_conw_r(g.conw_r)
+try:
+    g.scan(1, 3)
+    print("NO_ERROR")
+except ps.PeriodSearchError as e:
+    print("CODE", e.code)
+g.close()
+h = ps.PeriodSearch(sys.argv[2], form=ps.PS_FORM_FP64)
+h.set_conw_r(h.conw_r)
+rec = h.scan(1, 3)
+print("AFTER", int(all(rec["chi2"] > 0)))
+"""
+
+
+def test_bounded_wait_gives_up_and_reports(native, tmp_path):
+    """The tensor-core waits of the mixed kernel are bounded.  With the limit
+    set to zero polls (PS_B200_MAX_POLLS=0) every such wait gives up at
+    once: the kernel drains its own MMAs, frees its TMEM and returns, the scan
+    reports PS_ERR_DEVICE_LOOP, and the GPU context stays usable (an FP64
+    scan in the same process afterwards succeeds)."""
+    import subprocess
+    import sys
+
+    from conftest import REPO
+
+    script = tmp_path / "child.py"
+    script.write_text(_WAIT_CHILD)
+    env = dict(os.environ, PS_B200_MAX_POLLS="0")
+    r = subprocess.run([sys.executable, str(script), REPO, golden_path("tiny")], env=env, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "CODE %d" % native.PS_ERR_DEVICE_LOOP in r.stdout, r.stdout
+    assert "AFTER 1" in r.stdout, r.stdout
