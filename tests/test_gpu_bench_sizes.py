@@ -26,7 +26,7 @@ import numpy as np
 import pytest
 
 from conftest import GOLDEN, golden_path
-from test_gpu_parity import FIT_TOL, FORMS, _form, _read_full, check_records, perturbation_spread
+from test_gpu_parity import FIT_TOL, FORMS, _form, _read_full, check_records, perturbation_spread, perturbed_records
 
 sys.path.insert(0, GOLDEN)
 import make_golden  # noqa: E402  (the fixture definitions: inputs, periods)
@@ -41,17 +41,6 @@ def _fixture(name, *parts):
     return p
 
 
-def _spread_from(files, ref):
-    spread = np.zeros(len(ref), dtype=[("chi2", "f8"), ("lambda_deg", "f8"), ("beta_deg", "f8")])
-    for f in files:
-        if os.path.exists(f):
-            x = _read_full(f)
-            spread["chi2"] = np.maximum(spread["chi2"], np.abs(x["chi2"] - ref["chi2"]) / np.abs(ref["chi2"]))
-            for key in ("lambda_deg", "beta_deg"):
-                spread[key] = np.maximum(spread[key], np.abs(x[key] - ref[key]))
-    return spread
-
-
 @pytest.mark.parametrize("form", FORMS)
 def test_c2_spread_matches_reference(native, form):
     ref = _read_full(_fixture("c2", "ref_out.full"))
@@ -62,7 +51,7 @@ def test_c2_spread_matches_reference(native, form):
     conw_r = g.precalc()
     assert idx[0] == 1 and abs(conw_r * g.escl ** 2 - ref["dark_pct"][0]) <= 1e-12 * ref["dark_pct"][0]
     recs = np.concatenate([g.scan(n, n) for n in idx])
-    n_chaotic, worst = check_records(recs, ref, spread, "c2")
+    n_chaotic, worst = check_records(recs, ref, spread, "c2", perturbed_records("c2"))
     print(f"c2 {form}: {n_chaotic} chaotic of {len(ref)} periods, worst chi2 rel err {worst:.3e}")
     g.close()
 
@@ -86,9 +75,9 @@ def test_c4_shaped_batch_matches_restatement(native, tmp_path, form):
     for a, g in zip(meta["asteroids"], got):
         base = os.path.join(GOLDEN, "c4_shaped", "a%03d_" % a["index"])
         ref = _read_full(base + "oracle_out.full")
-        spread = _spread_from([base + "var_fma.full", base + "var_sq.full"], ref)
-        # the record's first line carries conw_r escl^2 in the restatement too
-        n_chaotic, worst = check_records(g, ref, spread, "c4_%d" % a["index"])
+        files = [base + "var_fma.full", base + "var_sq.full"]
+        spread = perturbation_spread("c4_shaped", ref, files)
+        n_chaotic, worst = check_records(g, ref, spread, "c4_%d" % a["index"], perturbed_records("c4_shaped", files))
         print(f"c4 asteroid {a['index']} ({a['n_points']} points) {form}: {n_chaotic} chaotic, worst {worst:.3e}")
     batch.close()
     for c in ctxs:
@@ -108,8 +97,7 @@ def test_c5_full_size_matches_restatement(native, tmp_path, form):
     n = meta["period"]
     got = g.scan(n, n)
     ref = _read_full(_fixture("c5", "oracle_out.full"))
-    spread = _spread_from([os.path.join(GOLDEN, "c5", "var_fma.full"), os.path.join(GOLDEN, "c5", "var_sq.full")],
-                          ref)
+    spread = perturbation_spread("c5", ref, ("var_fma.full", "var_sq.full"))
     err = abs(got["chi2"][0] - ref["chi2"][0]) / ref["chi2"][0]
     print(f"c5 {form}: chi2 rel err {err:.3e}, perturbation spread {spread['chi2'][0]:.3e}")
     assert err <= FIT_TOL or err <= 10 * spread["chi2"][0], (err, spread["chi2"][0])

@@ -107,24 +107,37 @@ def _read_full(path):
     return pso.read_full(path)
 
 
-def perturbation_spread(name, ref):
+PERTURBED = ("fma_out.full", "var_sq.full", "var_fma.full", "var_fmasq.full")
+
+
+def perturbed_records(name, files=PERTURBED):
+    """Records of the reference's last-ulp perturbations (its FMA rebuild and
+    the restatement's perturbed builds, tests/golden/make_golden.py)."""
+    paths = [f if os.path.isabs(f) else os.path.join(GOLDEN, name, f) for f in files]
+    return [_read_full(p) for p in paths if os.path.exists(p)]
+
+
+def perturbation_spread(name, ref, files=PERTURBED):
     """Largest change per period among last-ulp perturbations of the
-    reference (its FMA rebuild and the restatement's perturbed builds,
-    tests/golden/make_golden.py): relative for chi2, in degrees for the pole
-    angles, which a flat chi2 valley lets move further than chi2 does."""
+    reference: relative for chi2, in degrees for the pole angles, which a flat
+    chi2 valley lets move further than chi2 does."""
     spread = np.zeros(len(ref), dtype=[("chi2", "f8"), ("lambda_deg", "f8"), ("beta_deg", "f8")])
-    for f in ("fma_out.full", "var_sq.full", "var_fma.full", "var_fmasq.full"):
-        path = os.path.join(GOLDEN, name, f)
-        if os.path.exists(path):
-            x = _read_full(path)
-            spread["chi2"] = np.maximum(spread["chi2"], np.abs(x["chi2"] - ref["chi2"]) / np.abs(ref["chi2"]))
-            for key in ("lambda_deg", "beta_deg"):
-                spread[key] = np.maximum(spread[key], np.abs(x[key] - ref[key]))
+    for x in perturbed_records(name, files):
+        spread["chi2"] = np.maximum(spread["chi2"], np.abs(x["chi2"] - ref["chi2"]) / np.abs(ref["chi2"]))
+        for key in ("lambda_deg", "beta_deg"):
+            spread[key] = np.maximum(spread[key], np.abs(x[key] - ref[key]))
     return spread
 
 
-def check_records(gpu, ref, spread, label):
-    """Per-period parity with the chaotic-period triage, plus the ranking."""
+def _top(r, k):
+    return list(np.argsort(r["chi2"], kind="stable")[:k])
+
+
+def check_records(gpu, ref, spread, label, perturbed=()):
+    """Per-period parity with the chaotic-period triage, plus the ranking:
+    top-1/10/20 identical, except at a K where the reference's own last-ulp
+    perturbations (`perturbed` records) already reorder its top K -- there the
+    ranking is itself chaotic and only the per-period bar applies."""
     assert gpu.shape == ref.shape
     n = len(ref)
     cs = spread["chi2"]
@@ -147,7 +160,10 @@ def check_records(gpu, ref, spread, label):
         assert np.all(d[calm] <= tol[calm]), (key, [(int(i) + 1, float(d[i]), float(spread[key][i]))
                                                     for i in np.nonzero(calm & (d > tol))[0][:5]])
     for k in (1, min(10, n), min(20, n)):
-        assert list(np.argsort(gpu["chi2"], kind="stable")[:k]) == list(np.argsort(ref["chi2"], kind="stable")[:k])
+        if any(_top(x, k) != _top(ref, k) for x in perturbed):
+            print(f"{label}: top-{k} reordered by the reference's own perturbations; not compared")
+            continue
+        assert _top(gpu, k) == _top(ref, k), (label, k)
     return int(chaotic.sum()), float(err.max())
 
 
@@ -164,6 +180,6 @@ def test_scan_matches_reference(native, oracle_lib, name, form):
     recs = g.scan(1, len(ref))
     # the first record's 4th column is conw_r * escl^2 in the reference output
     assert abs(conw_r * g.escl * g.escl - ref["dark_pct"][0]) <= 1e-12 * ref["dark_pct"][0]
-    n_chaotic, worst = check_records(recs, ref, spread, name)
+    n_chaotic, worst = check_records(recs, ref, spread, name, perturbed_records(name))
     print(f"{name} {form}: {n_chaotic} chaotic periods of {len(ref)}, worst chi2 rel err {worst:.3e}")
     g.close()
