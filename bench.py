@@ -623,6 +623,8 @@ def main():
     same = times[:len(e2e_times)]
     e2e_extra = {"device_same_batches": world * fits_per_step * len(same) / sum(same) if same else None,
                  "phase_ms_median": {k: 1000 * statistics.median(v) for k, v in phases.items() if v},
+                 "step_ms": [round(1000 * t, 1) for t in e2e_times],
+                 "device_step_ms": [round(1000 * t, 1) for t in same],
                  "steps": len(e2e_times)}
 
     # the other numerical forms on the first timed batch (same periods, same

@@ -672,21 +672,30 @@ __device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, i
     curv_phase(P, a, g, area);
     __syncthreads();
     // chck and the facet-area sum, facets in order (as evaluate() and the
-    // fast point loop form them)
+    // fast point loop form them); four threads, loads ahead of the sums
     if (tid < 4) {
         double s = 0;
         if (tid < 3) {
-            for (int f = 0; f < F; f++) s = s + area[f] * P.fac[(size_t)f * 4 + tid];
+#pragma unroll 8
+            for (int f = 0; f < F; f++) s = s + area[f] * __ldg(P.fac + (size_t)f * 4 + tid);
             misc[M_CHK0 + tid] = s;
         } else {
+#pragma unroll 8
             for (int f = 0; f < F; f++) s = s + area[f];
             misc[M_SAREA] = s;
         }
     }
     const double cl = misc[M_CL], cls = misc[M_CLS];
-    for (int base = 0; base < P.n_points; base += kThreads) {
-        const int p = base + tid;
-        const bool act = p < P.n_points;
+    int* perm = (int*)(sm + L.perm);
+    // points in segments sorted by viewing direction (as in evaluate()), so
+    // that the points of a warp see nearly the same facets
+    for (int s0 = 0; s0 < P.n_points; s0 += P.sortseg) {
+    const int seg = min(P.sortseg, P.n_points - s0);
+    __syncthreads();
+    sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
+    for (int base = 0; base < seg; base += kThreads) {
+        const bool act = base + tid < seg;
+        const int p = act ? perm[base + tid] : 0;
         double e0_ = 0, e1_ = 0, e2_ = 0, f0_ = 0, f1_ = 0, f2_ = 0, sc = 0;
         if (act) {
             PointGeom G;
@@ -729,6 +738,7 @@ __device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, i
             }
         }
         if (act) yt[p] = br * sc;
+    }
     }
     __syncthreads();
     if (tid < 3) yt[P.n_points + tid] = misc[M_CHK0 + tid];
