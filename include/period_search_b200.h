@@ -228,7 +228,7 @@ int ps_format_record(const ps_record* r, int first_line, double conw_line, char*
  * in the reference (fixed array sizes there).
  * ps_autotune: time scans of trial periods 1..n (n = n_periods, at least
  * two waves of fits: 4 x SMs / 10 periods) under candidate
- * tiles (fch in {16, 32, 40, 48, 64}, rt in {16, 32, 64}; sortseg in {256, 1024}; the
+ * tiles (fch in {16, 32, 40, 48, 56, 64}, rt in {16, 32, 64}; sortseg in {256, 1024}; the
  * reference-order form only sortseg), keep the fastest; tiles[3] and
  * *seconds (its scan time) receive the choice. */
 int ps_set_tiles(ps_ctx* ctx, int fch, int rt, int sortseg);

@@ -128,9 +128,6 @@ int upload_mixed(ps_ctx* c) {
     const int F = p.numfac, C = p.ncoef;
     if (C > 64) return fail(PS_ERR_LIMIT, "the mixed form supports up to 64 shape coefficients (lmax <= 7)");
     const int nchunk = (F + 63) / 64;
-    std::vector<float> fac32((size_t)F * 4, 0.f);
-    for (int f = 0; f < F; f++)
-        for (int k = 0; k < 3; k++) fac32[(size_t)f * 4 + k] = (float)p.nor[(size_t)f * 3 + k];
     std::vector<uint16_t> bsw((size_t)nchunk * 2 * 64 * 64, 0);
     for (int ch = 0; ch < nchunk; ch++) {
         uint16_t* hi = &bsw[(size_t)ch * 2 * 4096];
@@ -146,11 +143,9 @@ int upload_mixed(ps_ctx* c) {
                 lo[off] = l;
             }
     }
-    PSB_CUDA(c->d_fac32.upload(fac32, c->stream));
     PSB_CUDA(c->d_bsw.upload(bsw, c->stream));
     PSB_CUDA(c->d_err.ensure(1));
     PSB_CUDA(cudaMemsetAsync(c->d_err.p, 0, sizeof(int), c->stream));
-    c->dp.fac32 = c->d_fac32.p;
     c->dp.bsw = c->d_bsw.p;
     c->dp.nchunk = nchunk;
     c->dp.err = c->d_err.p;
@@ -253,6 +248,11 @@ int upload_static(ps_ctx* c) {
         }
     }
     PSB_CUDA(c->d_fac.upload(fac, s));
+    // FP32 copies of the normals: the FP32 visibility pre-test and the mixed form
+    std::vector<float> fac32((size_t)F * 4, 0.f);
+    for (int f = 0; f < F; f++)
+        for (int k = 0; k < 3; k++) fac32[(size_t)f * 4 + k] = (float)p.nor[(size_t)f * 3 + k];
+    PSB_CUDA(c->d_fac32.upload(fac32, s));
     PSB_CUDA(c->d_dsph.upload(dsph, s));
     PSB_CUDA(c->d_cpl.upload(cpl, s));
     PSB_CUDA(c->d_cfc.upload(cfc, s));
@@ -305,6 +305,7 @@ int upload_static(ps_ctx* c) {
     d.lc_npts = c->d_lc.p + (L + 2) + (L + 1);
     d.free_idx = c->d_lc.p + lc.size();
     d.fac = c->d_fac.p;
+    d.fac32 = c->d_fac32.p;
     d.dsph = c->d_dsph.p;
     d.cpl = c->d_cpl.p;
     d.cfc = c->d_cfc.p;
@@ -693,7 +694,7 @@ int ps_autotune(ps_ctx* c, int n_periods, int* tiles, double* seconds) {
     if (rc) return rc;
     int best[3] = {start[0], start[1], start[2]};
     double tbest = 1e300;
-    static const int fchs[] = {16, 32, 40, 48, 64}, rts[] = {16, 32, 64}, segs[] = {256, 1024};
+    static const int fchs[] = {16, 32, 40, 48, 56, 64}, rts[] = {16, 32, 64}, segs[] = {256, 1024};
     for (int fch : fchs)
         for (int rt : rts)
             for (int seg : segs) {

@@ -210,6 +210,7 @@ int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out) {
             if (pa.lmax == po.lmax && pa.mmax == po.mmax && pa.nor == po.nor && pa.darea == po.darea &&
                 pa.dsph == po.dsph && pa.pleg == po.pleg && pa.fc == po.fc && pa.fs == po.fs) {
                 probs[a].fac = ctxs[o]->dp.fac;
+                probs[a].fac32 = ctxs[o]->dp.fac32;
                 probs[a].dsph = ctxs[o]->dp.dsph;
                 probs[a].cpl = ctxs[o]->dp.cpl;
                 probs[a].cfc = ctxs[o]->dp.cfc;

@@ -24,6 +24,16 @@ using namespace fitcommon;
 constexpr int kFch = 32;     // facets per shared-memory chunk (reference-order form)
 constexpr int kRt = 32;      // rows per alpha tile (reference-order form)
 constexpr int kMf = 128;     // facets per staged chunk of the model-only pass
+
+// Visibility pre-test in FP32.  A pair is visible when mu > 1e-8 and
+// mu0 > 1e-8 (bright.c:65) with mu, mu0 dot products of unit vectors in
+// FP64.  The same dot products in FP32, from FP32 copies of the unit vectors,
+// differ from the FP64 ones by at most ~3e-7 (three products of factors of
+// magnitude <= 1, each rounded to 2^-24 relative, plus the FP32 sums), so a
+// pair whose FP32 mu or mu0 is below kPreTest is invisible in FP64 as well;
+// only the other pairs are tested (and computed) in FP64.  The FP64
+// decision, and so every result, is unchanged.
+constexpr float kPreTest = -1e-6f;
 // The fast form takes its facet-chunk and alpha row-tile sizes and both forms
 // the point-sort segment from the problem (DevProblem::fch, rt, sortseg):
 // runtime tile shapes, chosen by ps_autotune; no choice changes any result.
@@ -41,9 +51,13 @@ __host__ __device__ constexpr int alpha_job_count(int mfit) {
     return n;
 }
 
+// Offset (doubles) in the work area of the damped matrix the Gauss-Jordan
+// solve starts from, after the solve's own buffers.
+__host__ __device__ constexpr int gj_covar_off(int mfit) { return (gj_buf_doubles(mfit) + 1) & ~1; }
+
 // Shared-memory layout, offsets in doubles.
 struct Layout {
-    int cg, atry, alpha, covar, beta, da, g, area, dres, dave, blm, misc, red, perm, work, ipiv, ent;
+    int cg, atry, alpha, beta, da, g, area, dres, dave, blm, misc, red, perm, work, ipiv, ent;
     size_t bytes;
 };
 
@@ -56,7 +70,6 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     PSB_TAKE(cg, P.ma)
     PSB_TAKE(atry, P.ma)
     PSB_TAKE(alpha, P.mfit * P.mfit)
-    PSB_TAKE(covar, P.mfit * P.mfit)
     PSB_TAKE(beta, P.mfit)
     PSB_TAKE(da, P.mfit)
     PSB_TAKE(g, P.F)
@@ -76,8 +89,10 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     int w = chunk > tile ? chunk : tile;
     if (P.mfit + 2 > w) w = P.mfit + 2;
     if (P.sortseg > w) w = P.sortseg;  // sort keys (uint64) before the point loop
-    if (3 * kMf > w) w = 3 * kMf;      // model-only pass: staged facet normals
-    if (gj_buf_doubles(P.mfit) > w) w = gj_buf_doubles(P.mfit);  // Gauss-Jordan buffers
+    if (5 * kMf > w) w = 5 * kMf;      // model-only pass: staged facet normals (FP64 + FP32)
+    // Gauss-Jordan: its buffers, then the damped matrix it starts from (covar),
+    // which it reads into registers -- covar needs no region of its own
+    if (gj_covar_off(P.mfit) + P.mfit * P.mfit > w) w = gj_covar_off(P.mfit) + P.mfit * P.mfit;
     PSB_TAKE(perm, P.sortseg / 2)
     PSB_TAKE(work, w)
 #undef PSB_TAKE
@@ -708,19 +723,28 @@ __device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, i
             f2_ = G.e0[2];
             sc = G.scale;
         }
+        const float ex = (float)e0_, ey = (float)e1_, ez = (float)e2_;
+        const float gx = (float)f0_, gy = (float)f1_, gz = (float)f2_;
         double br = 0;
+        double* nrm = work;                                   // [kMf][3] FP64 normals
+        float4* nrm32 = reinterpret_cast<float4*>(work + 3 * kMf);  // [kMf] FP32 normals
         for (int c0 = 0; c0 < F; c0 += kMf) {
             const int nf = min(kMf, F - c0);
             __syncthreads();
             for (int i = tid; i < nf * 3; i += kThreads) {
                 const int ff = i / 3, k = i - ff * 3;
-                work[i] = P.fac[(size_t)(c0 + ff) * 4 + k];
+                nrm[i] = P.fac[(size_t)(c0 + ff) * 4 + k];
             }
+            for (int ff = tid; ff < nf; ff += kThreads) nrm32[ff] = reinterpret_cast<const float4*>(P.fac32)[c0 + ff];
             __syncthreads();
             if (act) {
 #pragma unroll 4
                 for (int ff = 0; ff < nf; ff++) {
-                    const double nx = work[ff * 3 + 0], ny = work[ff * 3 + 1], nz = work[ff * 3 + 2];
+                    const float4 n32 = nrm32[ff];
+                    const float muf = fmaf(ex, n32.x, fmaf(ey, n32.y, ez * n32.z));
+                    const float mu0f = fmaf(gx, n32.x, fmaf(gy, n32.y, gz * n32.z));
+                    if (muf < kPreTest || mu0f < kPreTest) continue;
+                    const double nx = nrm[ff * 3 + 0], ny = nrm[ff * 3 + 1], nz = nrm[ff * 3 + 2];
                     const double mu = e0_ * nx + e1_ * ny + e2_ * nz;
                     const double mu0 = f0_ * nx + f1_ * ny + f2_ * nz;
                     if ((mu > kTinyD) && (mu0 > kTinyD)) {
@@ -1198,7 +1222,7 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
         // it after the last step.  Every value, and so every result, is the
         // same as with a full evaluation per step.
         double* alpha = sm + L.alpha;
-        double* covar = sm + L.covar;
+        double* covar = sm + L.work + gj_covar_off(mfit);  // free while no evaluation runs
         double* beta = sm + L.beta;
         double* da = sm + L.da;
         double alamda = -1, ochisq = 0, chisq = 0, iter_diff = 1e40, dev_old = 1e30, dev_new = 0, rchisq = -1;
