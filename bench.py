@@ -684,8 +684,12 @@ def main():
     # FP64 SIMT rate on B200), measured live on this GPU
     fp64_peak = ps.fp64_tensor_peak(local)
     achieved = flop_launch / t_launch / 1e12
+    # nominal FP64 tensor rate: SMs x 64 FMA/clk (m8n8k4 DMMA) x 2 FLOP x the
+    # maximum SM clock
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    theo = sms * 64 * 2 * (clocks.get("sm_max_mhz") or 1965.0) * 1e6 / 1e12
     roofline = {"bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp64_peak,
+                "frac": achieved / fp64_peak, "peak_theoretical": theo, "frac_of_theoretical": achieved / theo,
                 "peak_source": "FP64 tensor-core throughput (m8n8k4 MMA) measured live on this GPU; "
                                "the measured-peaks file holds bf16 and HBM figures only",
                 "traffic": None,
@@ -699,7 +703,7 @@ def main():
     # on the 300-fit profile launch of the c2 workload (bench.py --profile),
     # scaled to this launch's fits: the per-CTA J scratch (356 KB) stays in L2
     # at one fit per SM and is evicted at two
-    per_fit = {"fast": 5.66e7, "fp64": 5.20e6}.get(args.form) if args.config == "c2" else None
+    per_fit = {"fast": 2.39e7, "fp64": 5.20e6}.get(args.form) if args.config == "c2" else None
     if per_fit:
         roofline["traffic"] = per_fit * fits_per_step
         roofline["traffic_source"] = ("ncu dram bytes of the 300-fit c2 profile launch of this form, "

@@ -248,7 +248,7 @@ int upload_static(ps_ctx* c) {
         }
     }
     PSB_CUDA(c->d_fac.upload(fac, s));
-    // FP32 copies of the normals: the FP32 visibility pre-test and the mixed form
+    // FP32 copies of the normals (the mixed form reads them)
     std::vector<float> fac32((size_t)F * 4, 0.f);
     for (int f = 0; f < F; f++)
         for (int k = 0; k < 3; k++) fac32[(size_t)f * 4 + k] = (float)p.nor[(size_t)f * 3 + k];

@@ -31,7 +31,7 @@ struct DevProblem {
     // tile shapes (ps_set_tiles / ps_autotune): the fast form's facets per
     // staged chunk and alpha rows per tile, and the points sorted together
     int fch, rt, sortseg;
-    const float* fac32;          // [F][4]: nx, ny, nz, 0 (FP32 copies; all forms)
+    const float* fac32;          // [F][4]: nx, ny, nz, 0 (FP32 copies, mixed form)
     // mixed-precision form only
     const uint16_t* bsw;         // [nchunk][2][64 x 64] BF16 hi/lo of Dsph, swizzled K-major tiles
     int nchunk;                  // facet chunks of 64 (F padded up)

@@ -25,15 +25,20 @@ constexpr int kFch = 32;     // facets per shared-memory chunk (reference-order 
 constexpr int kRt = 32;      // rows per alpha tile (reference-order form)
 constexpr int kMf = 128;     // facets per staged chunk of the model-only pass
 
-// Visibility pre-test in FP32.  A pair is visible when mu > 1e-8 and
-// mu0 > 1e-8 (bright.c:65) with mu, mu0 dot products of unit vectors in
-// FP64.  The same dot products in FP32, from FP32 copies of the unit vectors,
-// differ from the FP64 ones by at most ~3e-7 (three products of factors of
-// magnitude <= 1, each rounded to 2^-24 relative, plus the FP32 sums), so a
-// pair whose FP32 mu or mu0 is below kPreTest is invisible in FP64 as well;
-// only the other pairs are tested (and computed) in FP64.  The FP64
-// decision, and so every result, is unchanged.
-constexpr float kPreTest = -1e-6f;
+constexpr int kMp = 4;       // points per thread at most in the model-only pass
+
+// 1/x for x in (2e-8, 2] (mu + mu0 of a visible pair), fast form only: the
+// hardware's approximate FP64 reciprocal refined by two Newton-Raphson steps
+// r <- r + r (1 - x r), each of which squares the relative error, so the
+// result is within rounding of the IEEE quotient.
+__device__ __forceinline__ double rcp_newton(double x) {
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
 // The fast form takes its facet-chunk and alpha row-tile sizes and both forms
 // the point-sort segment from the problem (DevProblem::fch, rt, sortseg):
 // runtime tile shapes, chosen by ps_autotune; no choice changes any result.
@@ -89,7 +94,7 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     int w = chunk > tile ? chunk : tile;
     if (P.mfit + 2 > w) w = P.mfit + 2;
     if (P.sortseg > w) w = P.sortseg;  // sort keys (uint64) before the point loop
-    if (5 * kMf > w) w = 5 * kMf;      // model-only pass: staged facet normals (FP64 + FP32)
+    if (4 * kMf > w) w = 4 * kMf;      // model-only pass: staged facet normals and areas
     // Gauss-Jordan: its buffers, then the damped matrix it starts from (covar),
     // which it reads into registers -- covar needs no region of its own
     if (gj_covar_off(P.mfit) + P.mfit * P.mfit > w) w = gj_covar_off(P.mfit) + P.mfit * P.mfit;
@@ -708,60 +713,67 @@ __device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, i
     const int seg = min(P.sortseg, P.n_points - s0);
     __syncthreads();
     sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
-    for (int base = 0; base < seg; base += kThreads) {
-        const bool act = base + tid < seg;
-        const int p = act ? perm[base + tid] : 0;
-        double e0_ = 0, e1_ = 0, e2_ = 0, f0_ = 0, f1_ = 0, f2_ = 0, sc = 0;
-        if (act) {
-            PointGeom G;
-            point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
-            e0_ = G.e[0];
-            e1_ = G.e[1];
-            e2_ = G.e[2];
-            f0_ = G.e0[0];
-            f1_ = G.e0[1];
-            f2_ = G.e0[2];
-            sc = G.scale;
+    // kMp points per thread at most (slot j of thread t: point base + j kThreads
+    // + t, so each slot's warp holds consecutive sorted points): independent
+    // chains per facet and one load of each facet for all of them
+    const int k = min(kMp, (seg + kThreads - 1) / kThreads);
+    for (int base = 0; base < seg; base += k * kThreads) {
+        int pj[kMp];
+        bool aj[kMp];
+        double ej[kMp][3], fj[kMp][3], sc[kMp], br[kMp];
+#pragma unroll
+        for (int j = 0; j < kMp; j++) {
+            const int i = base + j * kThreads + tid;
+            aj[j] = j < k && i < seg;
+            pj[j] = aj[j] ? perm[i] : 0;
+            br[j] = 0;
+            sc[j] = 0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) ej[j][c] = fj[j][c] = 0;
+            if (aj[j]) {
+                PointGeom G;
+                point_geometry(P, pj[j], B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    ej[j][c] = G.e[c];
+                    fj[j][c] = G.e0[c];
+                }
+                sc[j] = G.scale;
+            }
         }
-        const float ex = (float)e0_, ey = (float)e1_, ez = (float)e2_;
-        const float gx = (float)f0_, gy = (float)f1_, gz = (float)f2_;
-        double br = 0;
-        double* nrm = work;                                   // [kMf][3] FP64 normals
-        float4* nrm32 = reinterpret_cast<float4*>(work + 3 * kMf);  // [kMf] FP32 normals
+        double4* nrm = reinterpret_cast<double4*>(work);  // [kMf] nx, ny, nz, Area
         for (int c0 = 0; c0 < F; c0 += kMf) {
             const int nf = min(kMf, F - c0);
             __syncthreads();
-            for (int i = tid; i < nf * 3; i += kThreads) {
-                const int ff = i / 3, k = i - ff * 3;
-                nrm[i] = P.fac[(size_t)(c0 + ff) * 4 + k];
+            for (int ff = tid; ff < nf; ff += kThreads) {
+                const double* fa = P.fac + (size_t)(c0 + ff) * 4;
+                nrm[ff] = make_double4(fa[0], fa[1], fa[2], area[c0 + ff]);
             }
-            for (int ff = tid; ff < nf; ff += kThreads) nrm32[ff] = reinterpret_cast<const float4*>(P.fac32)[c0 + ff];
             __syncthreads();
-            if (act) {
-#pragma unroll 4
-                for (int ff = 0; ff < nf; ff++) {
-                    const float4 n32 = nrm32[ff];
-                    const float muf = fmaf(ex, n32.x, fmaf(ey, n32.y, ez * n32.z));
-                    const float mu0f = fmaf(gx, n32.x, fmaf(gy, n32.y, gz * n32.z));
-                    if (muf < kPreTest || mu0f < kPreTest) continue;
-                    const double nx = nrm[ff * 3 + 0], ny = nrm[ff * 3 + 1], nz = nrm[ff * 3 + 2];
-                    const double mu = e0_ * nx + e1_ * ny + e2_ * nz;
-                    const double mu0 = f0_ * nx + f1_ * ny + f2_ * nz;
+#pragma unroll 2
+            for (int ff = 0; ff < nf; ff++) {
+                const double4 n = nrm[ff];
+#pragma unroll
+                for (int j = 0; j < kMp; j++) {
+                    if (!aj[j]) continue;
+                    const double mu = ej[j][0] * n.x + ej[j][1] * n.y + ej[j][2] * n.z;
+                    const double mu0 = fj[j][0] * n.x + fj[j][1] * n.y + fj[j][2] * n.z;
                     if ((mu > kTinyD) && (mu0 > kTinyD)) {
-                        const double ar = area[c0 + ff];
                         if constexpr (kFast) {
-                            const double r = 1.0 / (mu + mu0);
-                            br = fma(ar, mu * mu0 * fma(cls, r, cl), br);
+                            const double r = rcp_newton(mu + mu0);
+                            br[j] = fma(n.w, mu * mu0 * fma(cls, r, cl), br[j]);
                         } else {
                             const double dnom = mu + mu0;
                             const double s = mu * mu0 * (cl + cls / dnom);
-                            br = br + ar * s;
+                            br[j] = br[j] + n.w * s;
                         }
                     }
                 }
             }
         }
-        if (act) yt[p] = br * sc;
+#pragma unroll
+        for (int j = 0; j < kMp; j++)
+            if (aj[j]) yt[pj[j]] = br[j] * sc[j];
     }
     }
     __syncthreads();
