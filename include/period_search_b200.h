@@ -110,12 +110,13 @@ typedef struct ps_ctx ps_ctx;
 int ps_open_file(const char* path, int device, int form, ps_ctx** out);
 /* Same from in-memory arrays (replaces CUDAPrepare + the host globals). */
 int ps_open(const ps_problem_desc* desc, int device, int form, ps_ctx** out);
-/* Release the context and its device memory (replaces CUDAUnprepare,
- * start_CUDA.h:14).  The context's large Jacobian work buffer goes back to a
- * per-device cache (a few buffers per device) for the next context, so that
- * opening a context per asteroid does not allocate and free it every time. */
+/* Release the context (replaces CUDAUnprepare, start_CUDA.h:14).  Its
+ * device buffers go back to a per-device cache (at most 512 buffers and
+ * 4 GiB per device) from which later contexts and batches draw, so that
+ * opening and closing a context per asteroid does not call cudaMalloc and
+ * the device-synchronising cudaFree every time. */
 void ps_close(ps_ctx* ctx);
-/* Free the cached work buffers of every device.  No counterpart in the
+/* Free the cached device buffers of every device.  No counterpart in the
  * reference (its buffers are static arrays). */
 void ps_release_cached_memory(void);
 

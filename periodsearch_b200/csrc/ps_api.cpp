@@ -5,6 +5,7 @@
 // and the period/pole loops of period_search/period_search_BOINC.cpp.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -52,16 +53,21 @@ struct PoolEntry {
 };
 std::mutex g_pool_mu;
 std::vector<PoolEntry> g_pool;
-constexpr int kPoolPerDevice = 4;
+constexpr int kPoolMaxBuffers = 512;
+constexpr size_t kPoolMaxBytes = 4ull << 30;
 }  // namespace
 
 cudaError_t pool_take(int device, size_t bytes, void** p, size_t* cap) {
+    if (bytes == 0) bytes = 1;
     {
         std::lock_guard<std::mutex> lk(g_pool_mu);
+        const size_t limit = std::max(2 * bytes, bytes + (1u << 20));
         int best = -1;
-        for (int i = 0; i < (int)g_pool.size(); i++)
-            if (g_pool[i].device == device && g_pool[i].cap >= bytes && (best < 0 || g_pool[i].cap < g_pool[best].cap))
+        for (int i = 0; i < (int)g_pool.size(); i++) {
+            const PoolEntry& e = g_pool[i];
+            if (e.device == device && e.cap >= bytes && e.cap <= limit && (best < 0 || e.cap < g_pool[best].cap))
                 best = i;
+        }
         if (best >= 0) {
             *p = g_pool[best].p;
             *cap = g_pool[best].cap;
@@ -77,22 +83,32 @@ cudaError_t pool_take(int device, size_t bytes, void** p, size_t* cap) {
 }
 
 void pool_give(int device, void* p, size_t cap) {
-    void* drop = nullptr;
+    std::vector<void*> drop;
     {
         std::lock_guard<std::mutex> lk(g_pool_mu);
         g_pool.push_back({device, p, cap});
-        int count = 0, smallest = -1;
-        for (int i = 0; i < (int)g_pool.size(); i++)
-            if (g_pool[i].device == device) {
+        for (;;) {
+            int count = 0, smallest = -1, largest = -1;
+            size_t bytes = 0;
+            for (int i = 0; i < (int)g_pool.size(); i++) {
+                if (g_pool[i].device != device) continue;
                 count++;
+                bytes += g_pool[i].cap;
                 if (smallest < 0 || g_pool[i].cap < g_pool[smallest].cap) smallest = i;
+                if (largest < 0 || g_pool[i].cap > g_pool[largest].cap) largest = i;
             }
-        if (count > kPoolPerDevice) {
-            drop = g_pool[smallest].p;
-            g_pool.erase(g_pool.begin() + smallest);
+            int victim = bytes > kPoolMaxBytes ? largest : (count > kPoolMaxBuffers ? smallest : -1);
+            if (victim < 0) break;
+            drop.push_back(g_pool[victim].p);
+            g_pool.erase(g_pool.begin() + victim);
         }
     }
-    if (drop) cudaFree(drop);
+    if (drop.empty()) return;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != device) cudaSetDevice(device);
+    for (void* q : drop) cudaFree(q);
+    if (cur != device) cudaSetDevice(cur);
 }
 }  // namespace psb
 
@@ -385,7 +401,7 @@ size_t scratch_stride(const ps_ctx* c) {
 
 int ensure_scratch(ps_ctx* c, int slots) {
     const size_t stride = scratch_stride(c);
-    PSB_CUDA(c->d_scratch.ensure(c->device, stride * slots));
+    PSB_CUDA(c->d_scratch.ensure(stride * slots));
     return PS_OK;
 }
 
@@ -580,7 +596,7 @@ void ps_close(ps_ctx* c) {
         c->d_lc.release();
         c->d_free.release();
         c->d_queue.release();
-        c->d_scratch.release(c->device);
+        c->d_scratch.release();
         c->d_fits.release();
         c->d_rec.release();
         c->d_eval.release();

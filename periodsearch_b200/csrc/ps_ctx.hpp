@@ -18,18 +18,38 @@ int set_error(int code, const std::string& msg);
 // Counts one kernel launch for ps_kernel_launches().
 void count_launch();
 
-// Grow-only device buffer.
+// Process-wide cache of device buffers per device.  Buffers released by a
+// context or batch (ps_close, ps_batch_close) go back to the cache and are
+// handed to the next request they fit (at most twice its size, or 1 MiB
+// more), so that opening and closing a context per asteroid does not pay a
+// cudaMalloc and a device-synchronising cudaFree for each of its tables and
+// its ~100 MB Jacobian scratch every time.  A buffer belongs to one owner at
+// a time.  The cache keeps at most kPoolMaxBuffers buffers and kPoolMaxBytes
+// per device, until ps_release_cached_memory or process exit.
+cudaError_t pool_take(int device, size_t bytes, void** p, size_t* cap);
+void pool_give(int device, void* p, size_t cap);
+
+// Grow-only device buffer on the device that is current when it first
+// allocates, drawn from and returned to the per-device cache.
 template <class T>
 struct DevBuf {
     T* p = nullptr;
     size_t n = 0;
+    int device = -1;
     cudaError_t ensure(size_t count) {
         if (count <= n) return cudaSuccess;
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
-        if (e == cudaSuccess) n = count;
+        release();
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e != cudaSuccess) return e;
+        void* q = nullptr;
+        size_t cap = 0;
+        e = pool_take(dev, count * sizeof(T), &q, &cap);
+        if (e == cudaSuccess) {
+            p = (T*)q;
+            n = cap / sizeof(T);
+            device = dev;
+        }
         return e;
     }
     cudaError_t upload(const std::vector<T>& v, cudaStream_t s) {
@@ -38,38 +58,6 @@ struct DevBuf {
         return cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
     }
     void release() {
-        if (p) cudaFree(p);
-        p = nullptr;
-        n = 0;
-    }
-};
-
-// Process-wide cache of large device work buffers per device.  A context
-// borrows one for its Jacobian scratch and returns it when it closes, so
-// that opening and closing a context per asteroid does not pay a cudaMalloc
-// and a device-synchronising cudaFree of ~100 MB each time.  A buffer
-// belongs to one context at a time; at most a few buffers per device stay
-// cached, until ps_release_cached_memory or process exit.
-cudaError_t pool_take(int device, size_t bytes, void** p, size_t* cap);
-void pool_give(int device, void* p, size_t cap);
-
-template <class T>
-struct PooledBuf {
-    T* p = nullptr;
-    size_t n = 0;
-    cudaError_t ensure(int device, size_t count) {
-        if (count <= n) return cudaSuccess;
-        release(device);
-        void* q = nullptr;
-        size_t cap = 0;
-        cudaError_t e = pool_take(device, count * sizeof(T), &q, &cap);
-        if (e == cudaSuccess) {
-            p = (T*)q;
-            n = cap / sizeof(T);
-        }
-        return e;
-    }
-    void release(int device) {
         if (p) pool_give(device, p, n * sizeof(T));
         p = nullptr;
         n = 0;
@@ -91,7 +79,7 @@ struct ps_ctx {
     // device tables
     psb::DevBuf<double> d_pts, d_rows, d_fac, d_dsph, d_cpl, d_cfc, d_cfs, d_cgf, d_pole;
     psb::DevBuf<int> d_lc, d_free, d_queue;
-    psb::PooledBuf<double> d_scratch;
+    psb::DevBuf<double> d_scratch;
     psb::DevBuf<psb::FitOut> d_fits;
     psb::DevBuf<ps_record> d_rec;
     psb::DevBuf<double> d_eval;
