@@ -17,10 +17,14 @@
 // The convexity rows (conv.c:12-29) are added explicitly.  Every reduction
 // runs in a fixed order, so results are deterministic.
 //
-// Kernels, in stream order: adj_setup (1 CTA: blmatrix, curv, z, convexity
-// rows), adj_points (thread per point), adj_rows (1 CTA: normalisation,
-// residuals, chi2, adjoint weights), adj_facets (thread per facet, blocks of
-// points), adj_final (1 CTA: the F x C contraction, non-shape columns).
+// Kernels, in stream order, each spread over the GPU: adj_curv (thread per
+// facet: blmatrix, curv, z), adj_conv (warp per convexity-row sum),
+// adj_points (thread per point), adj_lc (CTA per lightcurve: model and J v
+// sums), adj_rowsum (rows: normalised model, residual, u, per-CTA chi2),
+// adj_lck (CTA per lightcurve: the adjoint's y.u sum), adj_weights (thread
+// per point), adj_facets (thread per facet, blocks of points), adj_qs
+// (thread per facet), adj_cols (CTA per output column: the F x C
+// contraction and the non-shape columns), adj_out (the free parameters).
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -37,10 +41,11 @@ constexpr int kPtThreads = 128;  // adj_points: points per CTA
 constexpr int kFacetChunk = 256; // adj_points: facets staged per chunk
 constexpr int kFcThreads = 128;  // adj_facets: facets per CTA
 constexpr int kPtBlock = 512;    // adj_facets: points per CTA (staged)
+constexpr int kRowThreads = 256; // adj_rowsum: rows per CTA
 
 // misc slots
 enum { X_B = 0, X_D = 9, X_CL = 27, X_CLS = 28, X_OMG = 29, X_P1 = 30, X_P2 = 31, X_P3 = 32, X_CHK = 33,
-       X_CONVJV = 36, X_N = 40 };
+       X_N = 40 };
 
 __device__ double block_sum(double v, double* red) {
     // fixed-order tree: warp shuffles, then warp 0 over the warp partials
@@ -61,12 +66,14 @@ __device__ double block_sum(double v, double* red) {
     return s;
 }
 
-__global__ void adj_setup(const DevProblem* __restrict__ Pp, AdjWork W) {
+// blmatrix and the scattering/phase scalars (block 0), curv (curv.c:15-37)
+// and z = Dsph v, z0 = z without the first coefficient; thread per facet.
+__global__ void adj_curv(const DevProblem* __restrict__ Pp, AdjWork W) {
     const DevProblem& P = *Pp;
     const double* a = W.a;
-    const int tid = threadIdx.x, F = P.F, C = P.C, NCB = P.NCB;
+    const int C = P.C, NCB = P.NCB;
     double* x = W.misc;
-    if (tid == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         blmatrix(a[C], a[C + 1], x + X_B, x + X_D);
         x[X_CL] = exp(a[C + 6]);
         x[X_CLS] = a[C + 7];
@@ -75,55 +82,56 @@ __global__ void adj_setup(const DevProblem* __restrict__ Pp, AdjWork W) {
         x[X_P2] = a[C + 4];
         x[X_P3] = a[C + 5];
     }
-    // curv.c:15-37, and z = Dsph v, z0 = z without the first coefficient
-    for (int f = tid; f < F; f += blockDim.x) {
-        const double* pl = P.cpl + (size_t)f * P.nq;
-        const double* fc = P.cfc + (size_t)f * (P.mmax + 1);
-        const double* fs = P.cfs + (size_t)f * (P.mmax + 1);
-        double gi = 0;
-        int n = 0, q = 0;
-        for (int m = 0; m <= P.mmax; m++) {
-            for (int l = m; l <= P.lmax; l++) {
-                double fsum = a[n] * fc[m];
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= P.F) return;
+    const double* pl = P.cpl + (size_t)f * P.nq;
+    const double* fc = P.cfc + (size_t)f * (P.mmax + 1);
+    const double* fs = P.cfs + (size_t)f * (P.mmax + 1);
+    double gi = 0;
+    int n = 0, q = 0;
+    for (int m = 0; m <= P.mmax; m++) {
+        for (int l = m; l <= P.lmax; l++) {
+            double fsum = a[n] * fc[m];
+            n++;
+            if (m != 0) {
+                fsum = fma(a[n], fs[m], fsum);
                 n++;
-                if (m != 0) {
-                    fsum = fma(a[n], fs[m], fsum);
-                    n++;
-                }
-                gi = fma(pl[q], fsum, gi);
-                q++;
             }
-        }
-        gi = exp(gi);
-        W.g[f] = gi;
-        W.area[f] = P.fac[(size_t)f * 4 + 3] * gi;
-        double z = 0;
-        const double* ds = P.dsph + (size_t)f * NCB;
-        if (W.v)
-            for (int k = 1; k < C; k++) z = fma(ds[k], W.v[k], z);
-        W.z0[f] = z;
-        W.z[f] = W.v ? fma(ds[0], W.v[0], z) : 0.0;
-    }
-    __syncthreads();
-    // convexity rows: chck_nc = sum Area n_nc, dres_nc,k = sum Darea g Dsph_k n_nc
-    for (int job = tid; job < 3 + 3 * C; job += blockDim.x) {
-        double s = 0;
-        if (job < 3) {
-            for (int f = 0; f < F; f++) s = fma(W.area[f], P.fac[(size_t)f * 4 + job], s);
-            x[X_CHK + job] = s;
-        } else {
-            const int nc = (job - 3) / C, k = (job - 3) - nc * C;
-            for (int f = 0; f < F; f++)
-                s = fma(W.area[f] * P.dsph[(size_t)f * NCB + k], P.fac[(size_t)f * 4 + nc], s);
-            W.dres[nc * C + k] = s;
+            gi = fma(pl[q], fsum, gi);
+            q++;
         }
     }
-    __syncthreads();
-    if (tid < 3) {
-        double s = 0;
-        if (W.v)
-            for (int k = 0; k < C; k++) s = fma(W.dres[tid * C + k], W.v[k], s);
-        x[X_CONVJV + tid] = s;
+    gi = exp(gi);
+    W.g[f] = gi;
+    W.area[f] = P.fac[(size_t)f * 4 + 3] * gi;
+    double z = 0;
+    const double* ds = P.dsph + (size_t)f * NCB;
+    if (W.v)
+        for (int k = 1; k < C; k++) z = fma(ds[k], W.v[k], z);
+    W.z0[f] = z;
+    W.z[f] = W.v ? fma(ds[0], W.v[0], z) : 0.0;
+}
+
+// Convexity rows: chck_nc = sum Area n_nc and dres_nc,k = sum Darea g Dsph_k
+// n_nc; one warp per sum (lanes stride the facets, fixed-order shuffle tree).
+__global__ void adj_conv(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    const int F = P.F, C = P.C, NCB = P.NCB;
+    const int job = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (job >= 3 + 3 * C) return;
+    double s = 0;
+    if (job < 3) {
+        for (int f = lane; f < F; f += 32) s = fma(W.area[f], P.fac[(size_t)f * 4 + job], s);
+    } else {
+        const int nc = (job - 3) / C, k = (job - 3) - nc * C;
+        for (int f = lane; f < F; f += 32) s = fma(W.area[f] * P.dsph[(size_t)f * NCB + k], P.fac[(size_t)f * 4 + nc], s);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+        if (job < 3)
+            W.misc[X_CHK + job] = s;
+        else
+            W.dres[job - 3] = s;
     }
 }
 
@@ -212,41 +220,56 @@ __global__ void __launch_bounds__(kPtThreads) adj_points(const DevProblem* __res
     }
 }
 
-// Normalisation, residuals, chi2 and the adjoint weights; one CTA.
-__global__ void adj_rows(const DevProblem* __restrict__ Pp, AdjWork W) {
+// Lightcurve of data row r (binary search over the lightcurve starts).
+__device__ __forceinline__ int lc_of(const DevProblem& P, int r) {
+    int lo = 0, hi = P.n_lc - 2;  // the last lightcurve is the convexity pseudo-curve
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.lc_start[mid] <= r)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// Per relative lightcurve (one CTA each): ave = sum y, S = sum (J v without
+// v_1), coef = sig L / ave (mrqcof.c:53-58, 92-104).
+__global__ void adj_lc(const DevProblem* __restrict__ Pp, AdjWork W) {
     const DevProblem& P = *Pp;
     __shared__ double red[32];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int nlc = P.n_lc - 1;  // the last lightcurve is the convexity pseudo-curve
-    double* lc_ave = W.lcw;
-    double* lc_s = W.lcw + nlc;
-    double* lc_k = W.lcw + 2 * nlc;
-    double* lc_coef = W.lcw + 3 * nlc;
-    // per relative lightcurve: ave = sum y, S = sum (J v without v_1)
-    for (int lc = 0; lc < nlc; lc++) {
-        if (!P.lc_rel[lc]) continue;
-        const int r0 = P.lc_start[lc], r1 = P.lc_start[lc + 1];
-        double sy = 0, sj = 0;
-        for (int r = r0 + tid; r < r1; r += nt) {
-            sy += W.y[r];
-            sj += W.jv0[r];
-        }
-        sy = block_sum(sy, red);
-        sj = block_sum(sj, red);
-        if (tid == 0) {
-            lc_ave[lc] = sy;
-            lc_s[lc] = sj;
-            lc_coef[lc] = P.sig[r0] * (double)P.lc_npts[lc] / sy;
-        }
+    const int lc = blockIdx.x, nlc = P.n_lc - 1;
+    if (!P.lc_rel[lc]) return;
+    const int r0 = P.lc_start[lc], r1 = P.lc_start[lc + 1];
+    double sy = 0, sj = 0;
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+        sy += W.y[r];
+        sj += W.jv0[r];
     }
-    __syncthreads();
-    // rows: normalised model and J v, residual, u
+    sy = block_sum(sy, red);
+    sj = block_sum(sj, red);
+    if (threadIdx.x == 0) {
+        W.lcw[lc] = sy;
+        W.lcw[nlc + lc] = sj;
+        W.lcw[3 * nlc + lc] = P.sig[r0] * (double)P.lc_npts[lc] / sy;
+    }
+}
+
+// Rows: the normalised model and J v, the residual, u = W (y_obs - y') or
+// W J' v, and each CTA's share of chi2 (summed in block order by adj_cols).
+__global__ void adj_rowsum(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    __shared__ double red[32];
+    const int nlc = P.n_lc - 1;
+    const double* lc_ave = W.lcw;
+    const double* lc_s = W.lcw + nlc;
+    const double* lc_coef = W.lcw + 3 * nlc;
     double x2 = 0;
-    for (int r = tid; r < P.n_rows; r += nt) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < P.n_rows) {
         double yy, jv;
         if (r < P.n_points) {
-            int lc = 0;
-            while (P.lc_start[lc + 1] <= r) lc++;
+            const int lc = lc_of(P, r);
             if (P.lc_rel[lc]) {
                 const double coef = lc_coef[lc];
                 yy = coef * W.y[r];
@@ -256,40 +279,51 @@ __global__ void adj_rows(const DevProblem* __restrict__ Pp, AdjWork W) {
                 jv = W.jv[r];
             }
         } else {
-            yy = W.misc[X_CHK + (r - P.n_points)];
-            jv = W.misc[X_CONVJV + (r - P.n_points)];
+            // the convexity rows; their J v needs the C-term dot products
+            const int nc = r - P.n_points;
+            yy = W.misc[X_CHK + nc];
+            jv = 0;
+            if (W.v)
+                for (int k = 0; k < P.C; k++) jv = fma(W.dres[nc * P.C + k], W.v[k], jv);
         }
         const double w = P.sig2i[r] * P.wght[r];
         const double dy = P.yobs[r] - yy;
-        x2 = fma(dy * dy, w, x2);
+        x2 = dy * dy * w;
         W.u[r] = W.v ? w * jv : w * dy;
     }
     x2 = block_sum(x2, red);
-    if (tid == 0) *W.chi2 = x2;
-    // per relative lightcurve: kappa = sum y u / ave
-    for (int lc = 0; lc < nlc; lc++) {
-        if (!P.lc_rel[lc]) continue;
-        const int r0 = P.lc_start[lc], r1 = P.lc_start[lc + 1];
-        double s = 0;
-        for (int r = r0 + tid; r < r1; r += nt) s = fma(W.y[r], W.u[r], s);
-        s = block_sum(s, red);
-        if (tid == 0) lc_k[lc] = s / lc_ave[lc];
+    if (threadIdx.x == 0) W.x2part[blockIdx.x] = x2;
+}
+
+// Per relative lightcurve (one CTA each): kappa = sum y u / ave.
+__global__ void adj_lck(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    __shared__ double red[32];
+    const int lc = blockIdx.x, nlc = P.n_lc - 1;
+    if (!P.lc_rel[lc]) return;
+    const int r0 = P.lc_start[lc], r1 = P.lc_start[lc + 1];
+    double s = 0;
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) s = fma(W.y[r], W.u[r], s);
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) W.lcw[2 * nlc + lc] = s / W.lcw[lc];
+}
+
+// Adjoint weights per point: l (all columns), l0 (the first shape
+// coefficient, zero on relative rows); ls = l Scale for the facet pass.
+__global__ void adj_weights(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= P.n_points) return;
+    const int nlc = P.n_lc - 1;
+    const int lc = lc_of(P, r);
+    double l = W.u[r], l0 = l;
+    if (P.lc_rel[lc]) {
+        l = W.lcw[3 * nlc + lc] * (W.u[r] - W.lcw[2 * nlc + lc]);
+        l0 = 0.0;
     }
-    __syncthreads();
-    // adjoint weights per point: l (all columns), l0 (the first shape
-    // coefficient, zero on relative rows); ls = l Scale for the facet pass
-    for (int r = tid; r < P.n_points; r += nt) {
-        int lc = 0;
-        while (P.lc_start[lc + 1] <= r) lc++;
-        double l = W.u[r], l0 = l;
-        if (P.lc_rel[lc]) {
-            l = lc_coef[lc] * (W.u[r] - lc_k[lc]);
-            l0 = 0.0;
-        }
-        W.lam[r] = l;
-        W.ls[r] = l * W.scale[r];
-        W.ls0[r] = l0 * W.scale[r];
-    }
+    W.lam[r] = l;
+    W.ls[r] = l * W.scale[r];
+    W.ls0[r] = l0 * W.scale[r];
 }
 
 // q_f = sum_p ls_p s_pf and q0_f = sum_p ls0_p s_pf over a block of points;
@@ -324,37 +358,54 @@ __global__ void __launch_bounds__(kFcThreads) adj_facets(const DevProblem* __res
     W.q0[(size_t)blockIdx.y * P.F + f] = q0;
 }
 
-// out_k = sum_f Q_f Area_f Dsph_fk (Q0 for the first coefficient) + the
-// convexity rows; out_{C+j} = sum_p l_p J_p,C+j; then the free parameters.
-__global__ void adj_final(const DevProblem* __restrict__ Pp, AdjWork W) {
+// Q_f = Area_f sum over the point blocks of q (q0); thread per facet.
+__global__ void adj_qs(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= P.F) return;
+    double s = 0, s0 = 0;
+    for (int b = 0; b < W.npb; b++) {
+        s += W.q[(size_t)b * P.F + f];
+        s0 += W.q0[(size_t)b * P.F + f];
+    }
+    W.qs[f] = s * W.area[f];
+    W.qs0[f] = s0 * W.area[f];
+}
+
+// One CTA per output column k < C + 8: out_k = sum_f Q_f Dsph_fk (Q0 for the
+// first coefficient) + the convexity rows, out_{C+j} = sum_p l_p J_p,C+j;
+// block C + 8 sums the per-CTA chi2 shares in block order.
+__global__ void adj_cols(const DevProblem* __restrict__ Pp, AdjWork W) {
     const DevProblem& P = *Pp;
     __shared__ double red[32];
-    const int tid = threadIdx.x, nt = blockDim.x, F = P.F, C = P.C;
-    for (int f = tid; f < F; f += nt) {
-        double s = 0, s0 = 0;
-        for (int b = 0; b < W.npb; b++) {
-            s += W.q[(size_t)b * F + f];
-            s0 += W.q0[(size_t)b * F + f];
-        }
-        W.qs[f] = s * W.area[f];
-        W.qs0[f] = s0 * W.area[f];
-    }
-    __syncthreads();
-    for (int k = tid; k < C; k += nt) {
+    const int k = blockIdx.x, C = P.C, F = P.F;
+    double s = 0;
+    if (k < C) {
         const double* q = k == 0 ? W.qs0 : W.qs;
-        double s = 0;
-        for (int f = 0; f < F; f++) s = fma(q[f], P.dsph[(size_t)f * P.NCB + k], s);
-        for (int nc = 0; nc < 3; nc++) s = fma(W.dres[nc * C + k], W.u[P.n_points + nc], s);
-        W.full[k] = s;
+        for (int f = threadIdx.x; f < F; f += blockDim.x) s = fma(q[f], P.dsph[(size_t)f * P.NCB + k], s);
+    } else if (k < C + 8) {
+        const double* col = W.jns + (size_t)(k - C) * P.n_points;
+        for (int p = threadIdx.x; p < P.n_points; p += blockDim.x) s = fma(W.lam[p], col[p], s);
+    } else {
+        for (int b = threadIdx.x; b < W.nrb; b += blockDim.x) s += W.x2part[b];
     }
-    for (int j = 0; j < 8; j++) {
-        double s = 0;
-        for (int p = tid; p < P.n_points; p += nt) s = fma(W.lam[p], W.jns[(size_t)j * P.n_points + p], s);
-        s = block_sum(s, red);
-        if (tid == 0) W.full[C + j] = s;
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) {
+        if (k < C) {
+            for (int nc = 0; nc < 3; nc++) s = fma(W.dres[nc * C + k], W.u[P.n_points + nc], s);
+            W.full[k] = s;
+        } else if (k < C + 8) {
+            W.full[k] = s;
+        } else {
+            *W.chi2 = s;
+        }
     }
-    __syncthreads();
-    for (int i = tid; i < P.mfit; i += nt) W.out[i] = W.full[P.free_idx[i]];
+}
+
+// The free parameters' entries.
+__global__ void adj_out(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    for (int i = threadIdx.x; i < P.mfit; i += blockDim.x) W.out[i] = W.full[P.free_idx[i]];
 }
 
 }  // namespace
@@ -362,8 +413,9 @@ __global__ void adj_final(const DevProblem* __restrict__ Pp, AdjWork W) {
 size_t adjoint_work_doubles(const DevProblem& P) {
     const size_t N = P.n_points, F = P.F;
     const size_t npb = (N + kPtBlock - 1) / kPtBlock;
+    const size_t nrb = ((size_t)P.n_rows + kRowThreads - 1) / kRowThreads;
     return 2 * (size_t)P.ma + F * 7 + 3 * (size_t)P.C + X_N + N * (8 + 6 + 7) + P.n_rows + 4 * (size_t)P.n_lc +
-           2 * npb * F + 2 * (size_t)P.ma + 8;
+           2 * npb * F + 2 * (size_t)P.ma + 8 + nrb;
 }
 
 cudaError_t launch_adjoint(const DevProblem& P, const DevProblem* dP, double* work, const double* d_a,
@@ -402,13 +454,23 @@ cudaError_t launch_adjoint(const DevProblem& P, const DevProblem* dP, double* wo
     W.q = take((size_t)W.npb * F);
     W.q0 = take((size_t)W.npb * F);
     W.full = take(P.ma + 8);
+    W.nrb = (int)(((size_t)P.n_rows + kRowThreads - 1) / kRowThreads);
+    W.x2part = take((size_t)W.nrb);
     W.out = d_out;
     W.chi2 = d_chi2;
-    adj_setup<<<1, 256, 0, s>>>(dP, W);
+    const int nlc = P.n_lc - 1;
+    const unsigned fb = (unsigned)((F + 255) / 256);
+    adj_curv<<<fb, 256, 0, s>>>(dP, W);
+    adj_conv<<<(unsigned)((3 + 3 * P.C + 7) / 8), 256, 0, s>>>(dP, W);
     adj_points<<<(unsigned)((N + kPtThreads - 1) / kPtThreads), kPtThreads, 0, s>>>(dP, W);
-    adj_rows<<<1, 256, 0, s>>>(dP, W);
+    if (nlc > 0) adj_lc<<<(unsigned)nlc, 256, 0, s>>>(dP, W);
+    adj_rowsum<<<(unsigned)W.nrb, kRowThreads, 0, s>>>(dP, W);
+    if (nlc > 0) adj_lck<<<(unsigned)nlc, 256, 0, s>>>(dP, W);
+    adj_weights<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(dP, W);
     adj_facets<<<dim3((unsigned)((F + kFcThreads - 1) / kFcThreads), (unsigned)W.npb), kFcThreads, 0, s>>>(dP, W);
-    adj_final<<<1, 256, 0, s>>>(dP, W);
+    adj_qs<<<fb, 256, 0, s>>>(dP, W);
+    adj_cols<<<(unsigned)(P.C + 9), 256, 0, s>>>(dP, W);
+    adj_out<<<1, 128, 0, s>>>(dP, W);
     return cudaGetLastError();
 }
 

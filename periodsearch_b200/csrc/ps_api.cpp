@@ -870,7 +870,7 @@ static int run_adjoint(ps_ctx* c, const double* a, const double* v, double* chi2
         PSB_CUDA(cudaStreamSynchronize(c->stream));  // vf leaves scope
     }
     PSB_CUDA(psb::launch_adjoint(d, c->d_dp.p, d_work, d_a, v ? d_v : nullptr, d_out, d_chi2, c->stream));
-    for (int k = 0; k < 5; k++) psb::count_launch();
+    for (int k = 0; k < psb::kAdjointLaunches; k++) psb::count_launch();
     double x2 = 0;
     if (out) PSB_CUDA(cudaMemcpyAsync(out, d_out, d.mfit * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     PSB_CUDA(cudaMemcpyAsync(&x2, d_chi2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
