@@ -19,7 +19,8 @@
 //
 // Kernels, in stream order, each spread over the GPU: adj_curv (thread per
 // facet: blmatrix, curv, z), adj_conv (warp per convexity-row sum),
-// adj_points (thread per point), adj_lc (CTA per lightcurve: model and J v
+// adj_points (thread per point and facet slice), adj_points_fin (thread per
+// point: the slices' sums in order, the per-point results), adj_lc (CTA per lightcurve: model and J v
 // sums), adj_rowsum (rows: normalised model, residual, u, per-CTA chi2),
 // adj_lck (CTA per lightcurve: the adjoint's y.u sum), adj_weights (thread
 // per point), adj_facets (thread per facet, blocks of points), adj_qs
@@ -42,6 +43,17 @@ constexpr int kFacetChunk = 256; // adj_points: facets staged per chunk
 constexpr int kFcThreads = 128;  // adj_facets: facets per CTA
 constexpr int kPtBlock = 512;    // adj_facets: points per CTA (staged)
 constexpr int kRowThreads = 256; // adj_rowsum: rows per CTA
+constexpr int kPart = 11;        // adj_points: partial sums per point and facet slice
+constexpr int kMaxSlices = 8;    // adj_points: facet slices at most
+
+// Facet slices of the (point, facet) pass: enough CTAs to fill the GPU,
+// slices of at least 256 facets.
+inline int facet_slices(const DevProblem& P) {
+    const int pb = (P.n_points + kPtThreads - 1) / kPtThreads;
+    int s = 1;
+    while (s < kMaxSlices && pb * s < 4 * 148 && P.F / (2 * s) >= 256) s *= 2;
+    return s;
+}
 
 // misc slots
 enum { X_B = 0, X_D = 9, X_CL = 27, X_CLS = 28, X_OMG = 29, X_P1 = 30, X_P2 = 31, X_P3 = 32, X_CHK = 33,
@@ -135,23 +147,26 @@ __global__ void adj_conv(const DevProblem* __restrict__ Pp, AdjWork W) {
     }
 }
 
-// Per point: the model, the eight non-shape columns of J, the shape part of
-// J v (with and without the first coefficient), Scale, and e, e0 for the
-// adjoint pass.
+// Per point and facet slice: partial sums over the slice's facets of the
+// model brightness and of what the eight non-shape columns and the shape
+// part of J v need (br, Area s z, Area s z0, the Lambert / Lommel-Seeliger
+// sums, T = sum Area dsmu n, S = sum Area dsmu0 n); grid (point blocks,
+// facet slices), so that the (point, facet) pass fills the GPU.
 __global__ void __launch_bounds__(kPtThreads) adj_points(const DevProblem* __restrict__ Pp, AdjWork W) {
     const DevProblem& P = *Pp;
     __shared__ double sf[6][kFacetChunk];  // nx, ny, nz, Area, z, z0
-    const int tid = threadIdx.x, F = P.F, C = P.C;
+    const int tid = threadIdx.x, F = P.F, N = P.n_points;
     const int p = blockIdx.x * kPtThreads + tid;
-    const bool act = p < P.n_points;
+    const bool act = p < N;
+    const int per = (F + W.nfs - 1) / W.nfs;
+    const int fa0 = blockIdx.y * per, fa1 = min(F, fa0 + per);
     const double* x = W.misc;
     const double cl = x[X_CL], cls = x[X_CLS];
     PointGeom G;
     if (act) point_geometry(P, p, x + X_B, x + X_D, x[X_OMG], x[X_P1], x[X_P2], x[X_P3], G);
-    double br = 0, sz = 0, sz0 = 0, s_cl = 0, s_cls = 0;
-    double T0 = 0, T1 = 0, T2 = 0, S0 = 0, S1 = 0, S2 = 0;
-    for (int f0 = 0; f0 < F; f0 += kFacetChunk) {
-        const int nf = min(kFacetChunk, F - f0);
+    double acc[kPart] = {};
+    for (int f0 = fa0; f0 < fa1; f0 += kFacetChunk) {
+        const int nf = min(kFacetChunk, fa1 - f0);
         __syncthreads();
         for (int i = tid; i < nf; i += kPtThreads) {
             const double* fa = P.fac + (size_t)(f0 + i) * 4;
@@ -173,28 +188,50 @@ __global__ void __launch_bounds__(kPtThreads) adj_points(const DevProblem* __res
                 const double r = 1.0 / (mu + mu0);
                 const double s = mu * mu0 * fma(cls, r, cl);
                 const double t = ar * s;
-                br += t;
-                sz = fma(t, sf[4][i], sz);
-                sz0 = fma(t, sf[5][i], sz0);
+                acc[0] += t;                      // br
+                acc[1] = fma(t, sf[4][i], acc[1]);  // sum Area s z
+                acc[2] = fma(t, sf[5][i], acc[2]);  // sum Area s z0
                 const double q0 = mu0 * r, q1 = mu * r;
                 const double w = ar * fma(cls * q0, q0, cl * mu0);
                 const double w0 = ar * fma(cls * q1, q1, cl * mu);
-                T0 = fma(w, nx, T0);
-                T1 = fma(w, ny, T1);
-                T2 = fma(w, nz, T2);
-                S0 = fma(w0, nx, S0);
-                S1 = fma(w0, ny, S1);
-                S2 = fma(w0, nz, S2);
+                acc[3] = fma(w, nx, acc[3]);
+                acc[4] = fma(w, ny, acc[4]);
+                acc[5] = fma(w, nz, acc[5]);
+                acc[6] = fma(w0, nx, acc[6]);
+                acc[7] = fma(w0, ny, acc[7]);
+                acc[8] = fma(w0, nz, acc[8]);
                 const double mm = mu * mu0 * ar;
-                s_cl += mm;
-                s_cls = fma(mm, r, s_cls);
+                acc[9] += mm;                     // sum mu mu0 Area
+                acc[10] = fma(mm, r, acc[10]);    // sum mu mu0 Area / (mu + mu0)
             }
         }
     }
     if (!act) return;
+    for (int j = 0; j < kPart; j++) W.pp[((size_t)j * W.nfs + blockIdx.y) * N + p] = acc[j];
+}
+
+// Per point: the slices' partial sums in slice order, then the model, the
+// eight non-shape columns of J, the shape part of J v (with and without the
+// first coefficient), Scale, and e, e0 for the adjoint pass.
+__global__ void adj_points_fin(const DevProblem* __restrict__ Pp, AdjWork W) {
+    const DevProblem& P = *Pp;
+    const int N = P.n_points, C = P.C;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    const double* x = W.misc;
+    const double cl = x[X_CL];
+    PointGeom G;
+    point_geometry(P, p, x + X_B, x + X_D, x[X_OMG], x[X_P1], x[X_P2], x[X_P3], G);
+    double acc[kPart];
+    for (int j = 0; j < kPart; j++) {
+        double v = 0;
+        for (int k = 0; k < W.nfs; k++) v += W.pp[((size_t)j * W.nfs + k) * N + p];
+        acc[j] = v;
+    }
+    const double br = acc[0], sz = acc[1], sz0 = acc[2], s_cl = acc[9], s_cls = acc[10];
     const double sc = G.scale;
     double jn[8];
-    const double T[3] = {T0, T1, T2}, S[3] = {S0, S1, S2};
+    const double T[3] = {acc[3], acc[4], acc[5]}, S[3] = {acc[6], acc[7], acc[8]};
     for (int k = 0; k < 3; k++) {
         double v = 0;
         for (int j = 0; j < 3; j++) v = fma(T[j], G.de[j][k], fma(S[j], G.de0[j][k], v));
@@ -207,7 +244,7 @@ __global__ void __launch_bounds__(kPtThreads) adj_points(const DevProblem* __res
     jn[7] = sc * s_cls;
     double ns = 0;
     for (int j = 0; j < 8; j++) {
-        W.jns[(size_t)j * P.n_points + p] = jn[j];
+        W.jns[(size_t)j * N + p] = jn[j];
         if (W.v) ns = fma(jn[j], W.v[C + j], ns);
     }
     W.y[p] = br * sc;
@@ -215,8 +252,8 @@ __global__ void __launch_bounds__(kPtThreads) adj_points(const DevProblem* __res
     W.jv[p] = fma(sc, sz, ns);
     W.jv0[p] = fma(sc, sz0, ns);
     for (int c = 0; c < 3; c++) {
-        W.e6[(size_t)c * P.n_points + p] = G.e[c];
-        W.e6[(size_t)(3 + c) * P.n_points + p] = G.e0[c];
+        W.e6[(size_t)c * N + p] = G.e[c];
+        W.e6[(size_t)(3 + c) * N + p] = G.e0[c];
     }
 }
 
@@ -415,7 +452,7 @@ size_t adjoint_work_doubles(const DevProblem& P) {
     const size_t npb = (N + kPtBlock - 1) / kPtBlock;
     const size_t nrb = ((size_t)P.n_rows + kRowThreads - 1) / kRowThreads;
     return 2 * (size_t)P.ma + F * 7 + 3 * (size_t)P.C + X_N + N * (8 + 6 + 7) + P.n_rows + 4 * (size_t)P.n_lc +
-           2 * npb * F + 2 * (size_t)P.ma + 8 + nrb;
+           2 * npb * F + 2 * (size_t)P.ma + 8 + nrb + (size_t)kPart * kMaxSlices * N;
 }
 
 cudaError_t launch_adjoint(const DevProblem& P, const DevProblem* dP, double* work, const double* d_a,
@@ -456,13 +493,16 @@ cudaError_t launch_adjoint(const DevProblem& P, const DevProblem* dP, double* wo
     W.full = take(P.ma + 8);
     W.nrb = (int)(((size_t)P.n_rows + kRowThreads - 1) / kRowThreads);
     W.x2part = take((size_t)W.nrb);
+    W.nfs = facet_slices(P);
+    W.pp = take((size_t)kPart * W.nfs * N);
     W.out = d_out;
     W.chi2 = d_chi2;
     const int nlc = P.n_lc - 1;
     const unsigned fb = (unsigned)((F + 255) / 256);
     adj_curv<<<fb, 256, 0, s>>>(dP, W);
     adj_conv<<<(unsigned)((3 + 3 * P.C + 7) / 8), 256, 0, s>>>(dP, W);
-    adj_points<<<(unsigned)((N + kPtThreads - 1) / kPtThreads), kPtThreads, 0, s>>>(dP, W);
+    adj_points<<<dim3((unsigned)((N + kPtThreads - 1) / kPtThreads), (unsigned)W.nfs), kPtThreads, 0, s>>>(dP, W);
+    adj_points_fin<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(dP, W);
     if (nlc > 0) adj_lc<<<(unsigned)nlc, 256, 0, s>>>(dP, W);
     adj_rowsum<<<(unsigned)W.nrb, kRowThreads, 0, s>>>(dP, W);
     if (nlc > 0) adj_lck<<<(unsigned)nlc, 256, 0, s>>>(dP, W);

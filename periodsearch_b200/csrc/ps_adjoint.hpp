@@ -26,12 +26,13 @@ struct AdjWork {
     double* out;                           // [mfit] result over the free parameters
     double* chi2;                          // [1]
     double* x2part;                        // [nrb] chi2 per row block
-    int npb, nrb;
+    double* pp;                            // [11][nfs][N] per-slice partial sums of the point pass
+    int npb, nrb, nfs;
 };
 
 size_t adjoint_work_doubles(const DevProblem& P);
 // Kernel launches of one launch_adjoint call.
-constexpr int kAdjointLaunches = 11;
+constexpr int kAdjointLaunches = 12;
 // chi2 into d_chi2; d_v == nullptr: beta = J^T W (y_obs - y) into d_out,
 // else J^T W (J v) (v over all ma parameters, zero on the fixed ones).
 cudaError_t launch_adjoint(const DevProblem& P, const DevProblem* dP, double* work, const double* d_a,
