@@ -209,73 +209,97 @@ void sphfunc(Problem& p) {
     }
 }
 
-// ludcmp.c:9-68 on an n x n row-major matrix (0-based storage).
-int ludcmp(std::vector<double>& a, int n, std::vector<int>& indx) {
-    std::vector<double> v(n + 1);
-    auto Aij = [&](int i, int j) -> double& { return a[(size_t)(i - 1) * n + (j - 1)]; };
-    indx.assign(n + 1, 0);
-    int imax = -999;
-    for (int i = 1; i <= n; i++) {
-        double big = 0.0, temp;
-        for (int j = 1; j <= n; j++)
-            if ((temp = std::fabs(Aij(i, j))) > big) big = temp;
-        if (big == 0.0) return 4;
-        v[i] = 1.0 / big;
-    }
-    for (int j = 1; j <= n; j++) {
-        for (int i = 1; i < j; i++) {
-            double sum = Aij(i, j);
-            for (int k = 1; k < i; k++) sum -= Aij(i, k) * Aij(k, j);
-            Aij(i, j) = sum;
-        }
-        double big = 0.0, dum;
-        for (int i = j; i <= n; i++) {
-            double sum = Aij(i, j);
-            for (int k = 1; k < j; k++) sum -= Aij(i, k) * Aij(k, j);
-            Aij(i, j) = sum;
-            if ((dum = v[i] * std::fabs(sum)) >= big) {
-                big = dum;
-                imax = i;
-            }
-        }
-        if (j != imax) {
-            for (int k = 1; k <= n; k++) {
-                dum = Aij(imax, k);
-                Aij(imax, k) = Aij(j, k);
-                Aij(j, k) = dum;
-            }
-            v[imax] = v[j];
-        }
-        indx[j] = imax;
-        if (Aij(j, j) == 0.0) Aij(j, j) = 1.0e-20;
-        if (j != n) {
-            dum = 1.0 / (Aij(j, j));
-            for (int i = j + 1; i <= n; i++) Aij(i, j) *= dum;
-        }
-    }
-    return 0;
-}
+// Dense LU solve of the ellipsoid fit's normal equations, the role of the
+// reference's ludcmp/lubksb (ludcmp.c:9-68, lubksb.c:3-24), written from the
+// algorithm: Crout's LU factorisation P A = L U with implicit row scaling and
+// partial pivoting, then forward and back substitution.  The result must
+// carry the reference's bits (cg_first seeds every fit), so the choices that
+// decide rounding are the reference's: columns are processed left to right,
+// each entry's dot product is subtracted term by term in index order, the
+// pivot of a column is the row maximising |entry| / (largest |entry| of its
+// original row), the last such row on ties, rows are exchanged whole, a zero
+// pivot becomes 1e-20, the multipliers below the pivot are formed with the
+// pivot's reciprocal, and forward substitution starts at the first nonzero
+// right-hand-side entry.
+struct LuSolver {
+    int n = 0;
+    std::vector<double> m;   // row-major; L below the diagonal (unit), U on and above
+    std::vector<int> swap;   // row exchanged with row j at column j
+    std::vector<double> rinv;  // 1 / (largest |entry| of each row), permuted with the rows
 
-// lubksb.c:3-24; b is 1-based (b[0] unused).
-void lubksb(const std::vector<double>& a, int n, const std::vector<int>& indx, std::vector<double>& b) {
-    auto Aij = [&](int i, int j) { return a[(size_t)(i - 1) * n + (j - 1)]; };
-    int ii = 0;
-    for (int i = 1; i <= n; i++) {
-        int ip = indx[i];
-        double sum = b[ip];
-        b[ip] = b[i];
-        if (ii)
-            for (int j = ii; j <= i - 1; j++) sum -= Aij(i, j) * b[j];
-        else if (sum)
-            ii = i;
-        b[i] = sum;
+    // Returns 4 (the reference's exit code) when a row is entirely zero.
+    int factor(const std::vector<double>& a, int size) {
+        n = size;
+        m = a;
+        swap.assign(n, 0);
+        rinv.assign(n, 0.0);
+        for (int r = 0; r < n; r++) {
+            double largest = 0.0;
+            for (int c = 0; c < n; c++) {
+                const double v = std::fabs(at(r, c));
+                if (v > largest) largest = v;
+            }
+            if (largest == 0.0) return 4;
+            rinv[r] = 1.0 / largest;
+        }
+        int pivot_row = -1;  // kept across columns, as a column of NaNs leaves it
+        for (int col = 0; col < n; col++) {
+            for (int r = 0; r < col; r++) at(r, col) = reduced(r, col, r);
+            double best = 0.0;
+            for (int r = col; r < n; r++) {
+                const double v = reduced(r, col, col);
+                at(r, col) = v;
+                const double score = rinv[r] * std::fabs(v);
+                if (score >= best) {
+                    best = score;
+                    pivot_row = r;
+                }
+            }
+            if (pivot_row != col) {
+                for (int c = 0; c < n; c++) std::swap(at(pivot_row, c), at(col, c));
+                rinv[pivot_row] = rinv[col];
+            }
+            swap[col] = pivot_row;
+            if (at(col, col) == 0.0) at(col, col) = 1.0e-20;
+            if (col + 1 < n) {
+                const double inv = 1.0 / at(col, col);
+                for (int r = col + 1; r < n; r++) at(r, col) *= inv;
+            }
+        }
+        return 0;
     }
-    for (int i = n; i >= 1; i--) {
-        double sum = b[i];
-        for (int j = i + 1; j <= n; j++) sum -= Aij(i, j) * b[j];
-        b[i] = sum / Aij(i, i);
+
+    // Solves A x = rhs in place (rhs has n entries).
+    void solve(std::vector<double>& rhs) const {
+        int first = -1;  // first row with a nonzero right-hand side after the exchanges
+        for (int r = 0; r < n; r++) {
+            double v = rhs[swap[r]];
+            rhs[swap[r]] = rhs[r];
+            if (first >= 0) {
+                for (int c = first; c < r; c++) v -= get(r, c) * rhs[c];
+            } else if (v != 0.0) {
+                first = r;
+            }
+            rhs[r] = v;
+        }
+        for (int r = n - 1; r >= 0; r--) {
+            double v = rhs[r];
+            for (int c = r + 1; c < n; c++) v -= get(r, c) * rhs[c];
+            rhs[r] = v / get(r, r);
+        }
     }
-}
+
+  private:
+    double& at(int r, int c) { return m[(size_t)r * n + c]; }
+    double get(int r, int c) const { return m[(size_t)r * n + c]; }
+    // entry (r, c) minus the dot product of row r of L and column c of U over
+    // the first `terms` indices, subtracted term by term
+    double reduced(int r, int c, int terms) const {
+        double v = get(r, c);
+        for (int k = 0; k < terms; k++) v -= get(r, k) * get(k, c);
+        return v;
+    }
+};
 
 // ellfit.c:11-88: Laplace-series coefficients of the ellipsoid's log
 // curvature function (normal equations + LU solve).
@@ -305,7 +329,7 @@ int ellfit(Problem& p) {
                 }
             }
     }
-    std::vector<double> fitmat((size_t)C * C), fitvec(C + 1);
+    std::vector<double> fitmat((size_t)C * C), fitvec(C);
     for (int i = 0; i < C; i++) {
         for (int j = 0; j < C; j++) {
             double s = 0;
@@ -314,13 +338,12 @@ int ellfit(Problem& p) {
         }
         double s = 0;
         for (int j = 0; j < F; j++) s = s + fmat[(size_t)j * C + i] * er[j];
-        fitvec[i + 1] = s;
+        fitvec[i] = s;
     }
-    std::vector<int> indx;
-    if (ludcmp(fitmat, C, indx) != 0) return 4;
-    lubksb(fitmat, C, indx, fitvec);
-    p.cg_first.assign(C, 0);
-    for (int i = 0; i < C; i++) p.cg_first[i] = fitvec[i + 1];
+    LuSolver lu;
+    if (lu.factor(fitmat, C) != 0) return 4;
+    lu.solve(fitvec);
+    p.cg_first = fitvec;
     return 0;
 }
 
