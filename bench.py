@@ -300,6 +300,10 @@ def _c4_worker(args):
 
 
 def run_c4(args, local):
+    print(json.dumps(c4_measure(args, local)), flush=True)
+
+
+def c4_measure(args, local):
     """Uneven multi-asteroid batch: many asteroids, point counts
     log-uniform in 100-5000, dense/sparse mix, lmax = 6, nrows = 10,
     per-fit convergence, all in one persistent launch replayed from a CUDA
@@ -393,7 +397,76 @@ def run_c4(args, local):
     batch.close()
     for c in ctxs:
         c.close()
-    print(json.dumps(line), flush=True)
+    # end to end through the public API: open every asteroid from its input
+    # file (host setup and uploads on host threads), open the batch, scan the
+    # step's periods into host records, close everything
+    e2e_times = []
+    h2d = sum(os.path.getsize(p) for p, _ in made)
+    for s in range(0 if getattr(args, "no_e2e", False) else 1):
+        a, b = ranges(args.warmup + s)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        cs = ps.open_many([p for p, _ in made], device=local, form=form, conw_r="start")
+        bt = ps.PeriodSearchBatch(cs)
+        recs = bt.scan(a, b)
+        bt.close()
+        for c in cs:
+            c.close()
+        e2e_times.append(time.perf_counter() - t0)
+    if e2e_times:
+        n_rec = sum(len(r) for r in recs)
+        line["e2e"] = {"value": fits / args.steps * len(e2e_times) / sum(e2e_times), "unit": "fits/s",
+                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(n_rec * 48),
+                       "what": "per step: open all asteroids from their input files, open the batch (graph "
+                               "capture), scan, records to host, close",
+                       "step_ms": [round(1000 * t, 1) for t in e2e_times]}
+    return line
+
+
+def extra_workloads(args, local):
+    """The uneven 512-asteroid batch (c4) and the 20 000-point lmax 8 shape
+    (c5), each one warm-up and one timed step with the default tiles, so that
+    every bench run records them beside the headline."""
+    import types
+
+    import torch
+
+    import periodsearch_b200 as ps
+
+    out = {}
+    try:
+        a = types.SimpleNamespace(form=args.form if args.form in ("fp64", "fast") else "fast", asteroids=512,
+                                  c4_periods=4, steps=1, warmup=1, no_autotune=True, no_e2e=True)
+        line = c4_measure(a, local)
+        out["c4"] = {k: line[k] for k in ("value", "unit", "ms_per_step", "per_asteroid_ms", "gpu_launches")}
+        out["c4"]["workload"] = line["config"]["workload"]
+        out["c4"]["setup_s"] = line["config"]["setup"]["seconds"]
+    except Exception as e:  # recorded, not fatal: the headline line still prints
+        out["c4"] = {"error": repr(e)[:300]}
+    try:
+        path = make_input(tempfile.mkdtemp(prefix="psc5"), "c5")
+        g = ps.PeriodSearch(path, device=local, form=ps.PS_FORM_FAST)
+        g.set_conw_r(g.conw_r)
+        B = 14
+        d = torch.zeros(B * 6, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.Stream()
+        g.scan_device(1, B, d.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        g.scan_device(1 + B, 2 * B, d.data_ptr(), stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1000.0
+        fl = 10 * B * 51 * flop_per_eval(g.n_points, g.numfac, g.ncoef, g.mfit)
+        out["c5"] = {"value": 10 * B / t, "unit": "fits/s", "ms_per_step": 1000 * t, "tflops": fl / t / 1e12,
+                     "frac_of_fp64_peak": fl / t / 1e12 / ps.fp64_tensor_peak(local), "workload": WORKLOAD_C5,
+                     "fits_per_step": 10 * B}
+        g.close()
+    except Exception as e:
+        out["c5"] = {"error": repr(e)[:300]}
+    return out
 
 
 def initial_parameters(g, freq, pole):
@@ -477,6 +550,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip timing the other numerical forms on one batch")
+    ap.add_argument("--no-extra", action="store_true", help="skip the one-step c4 and c5 measurements")
     ap.add_argument("--config", default="c2", choices=["c2", "c4", "c5"],
                     help="c2: production sparse search (the headline); c4: uneven multi-asteroid batch; "
                          "c5: lmax 8 / 2048 facets / 20000 points (14 periods per step, no pre-pass)")
@@ -491,7 +565,7 @@ def main():
         args.periods_per_step = min(args.periods_per_step, 14)
     if args.profile:
         args.periods_per_step = 30
-        args.no_cpu = args.no_e2e = args.no_forms = True
+        args.no_cpu = args.no_e2e = args.no_forms = args.no_extra = True
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -745,6 +819,8 @@ def main():
             line["cpu_baseline"] = {"value": v, "unit": "fits/s", "cores": cores, "kind": "port",
                                     "sample": sample + (f"; {why}" if why else "")}
     g.close()
+    if rank == 0 and world == 1 and not args.no_extra and args.config == "c2":
+        line["other_workloads"] = extra_workloads(args, local)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
