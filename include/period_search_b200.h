@@ -140,7 +140,8 @@ int ps_scan(ps_ctx* ctx, int n_from, int n_to, ps_record* out);
  * context's tables are complete on the device when ps_open* and
  * ps_precalc / ps_set_conw_r return, so any stream may scan afterwards.
  * Scans of one context share its work buffers: scans on different streams
- * must not overlap on the GPU. */
+ * must not overlap on the GPU.  ps_close waits for the last scan launched on
+ * a caller's stream before it releases the context. */
 int ps_scan_device(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, void* stream);
 
 /* ps_scan_device without any device-memory allocation.  No counterpart in

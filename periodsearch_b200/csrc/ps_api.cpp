@@ -43,6 +43,12 @@ int cuda_fail(cudaError_t e, const char* where) {
 
 namespace psb {
 int set_error(int code, const std::string& msg) { return fail(code, msg); }
+
+cudaError_t note_caller_stream(ps_ctx* c, cudaStream_t s) {
+    if (s == c->stream || !c->caller_done) return cudaSuccess;
+    c->caller_pending = true;
+    return cudaEventRecord(c->caller_done, s);
+}
 void count_launch() { g_launches++; }
 
 namespace {
@@ -445,6 +451,7 @@ int open_device(ps_ctx* c, int device) {
     c->device = device;
     PSB_CUDA(cudaSetDevice(device));
     PSB_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    PSB_CUDA(cudaEventCreateWithFlags(&c->caller_done, cudaEventDisableTiming));
     PSB_CUDA(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
     c->host_only = false;
     int rc = upload_static(c);
@@ -584,6 +591,7 @@ void ps_close(ps_ctx* c) {
     if (!c->host_only) {
         cudaSetDevice(c->device);
         if (c->stream) cudaStreamSynchronize(c->stream);
+        if (c->caller_pending) cudaEventSynchronize(c->caller_done);
         c->d_pts.release();
         c->d_rows.release();
         c->d_fac.release();
@@ -606,6 +614,7 @@ void ps_close(ps_ctx* c) {
         c->d_bsw.release();
         c->d_err.release();
         if (c->stream) cudaStreamDestroy(c->stream);
+        if (c->caller_done) cudaEventDestroy(c->caller_done);
     }
     delete c;
 }
@@ -748,7 +757,9 @@ int ps_scan_device(ps_ctx* c, int n_from, int n_to, ps_record* d_out, void* stre
     if (stream) c->stream = (cudaStream_t)stream;
     rc = scan_into(c, n_from, n_to, d_out, 0);
     c->stream = saved;
-    return rc;
+    if (rc) return rc;
+    if (stream) PSB_CUDA(psb::note_caller_stream(c, (cudaStream_t)stream));
+    return PS_OK;
 }
 
 int ps_scan(ps_ctx* c, int n_from, int n_to, ps_record* out) {

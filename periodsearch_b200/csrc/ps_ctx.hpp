@@ -15,6 +15,9 @@ namespace psb {
 
 // Records the message returned by ps_last_error() for the calling thread.
 int set_error(int code, const std::string& msg);
+// After a launch on stream s: if s is not the context's own stream, record
+// the context's caller_done event on it (no allocation).
+cudaError_t note_caller_stream(ps_ctx* c, cudaStream_t s);
 // Counts one kernel launch for ps_kernel_launches().
 void count_launch();
 
@@ -73,6 +76,10 @@ struct ps_ctx {
     bool host_only = true;
     bool rows_ready = false;
     cudaStream_t stream = nullptr;
+    // recorded after each scan launched on a caller's stream: ps_close waits
+    // for it before the context's buffers go back to the cache
+    cudaEvent_t caller_done = nullptr;
+    bool caller_pending = false;
     int sms = 0, blocks_per_sm = 0;
     int prepass_fits = 0;  // fits run by the last ps_precalc
     psb::DevProblem dp{};

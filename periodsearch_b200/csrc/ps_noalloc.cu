@@ -109,5 +109,7 @@ extern "C" int ps_scan_device_noalloc(ps_ctx* c, int n_from, int n_to, ps_record
     e = psb::launch_period_reduce(fits, np, d.ndata_m3, 0, d_out, s);
     if (e != cudaSuccess) return psb::set_error(PS_ERR_CUDA, cudaGetErrorString(e));
     psb::count_launch();
+    e = psb::note_caller_stream(c, s);  // records an event created at open: no allocation
+    if (e != cudaSuccess) return psb::set_error(PS_ERR_CUDA, cudaGetErrorString(e));
     return PS_OK;
 }
