@@ -365,11 +365,10 @@ int upload_static(ps_ctx* c) {
 
 // Data rows for a given conw_r: the 3 convexity rows have brightness 0,
 // sigma 1/conw_r and weight 1 (period_search_BOINC.cpp:491-496, 444-456).
-int upload_rows(ps_ctx* c) {
-    Problem& p = c->prob;
+// rows: yobs, sig, sig2i, weight, each n_points + 3 long.
+void build_rows(const Problem& p, double conw_r, double* rows) {
     const int N = p.n_points, R = N + 3;
-    std::vector<double> rows((size_t)4 * R);
-    double* yobs = rows.data();
+    double* yobs = rows;
     double* sig = yobs + R;
     double* sig2i = sig + R;
     double* wght = sig2i + R;
@@ -380,10 +379,17 @@ int upload_rows(ps_ctx* c) {
     }
     for (int j = 0; j < 3; j++) {
         yobs[N + j] = 0;
-        sig[N + j] = 1 / p.conw_r;
+        sig[N + j] = 1 / conw_r;
         wght[N + j] = 1;
     }
     for (int i = 0; i < R; i++) sig2i[i] = 1 / (sig[i] * sig[i]);  // mrqcof.c:113
+}
+
+int upload_rows(ps_ctx* c) {
+    Problem& p = c->prob;
+    const int N = p.n_points, R = N + 3;
+    std::vector<double> rows((size_t)4 * R);
+    build_rows(p, p.conw_r, rows.data());
     PSB_CUDA(c->d_rows.upload(rows, c->stream));
     c->dp.yobs = c->d_rows.p;
     c->dp.sig = c->d_rows.p + R;
@@ -619,6 +625,64 @@ void ps_close(ps_ctx* c) {
     delete c;
 }
 
+// The fits of several convexity pre-pass rounds in one launch, round k with
+// convexity weight cw[k]: every round's fits read their own copy of the
+// problem (the rows differ only in the convexity rows' sigma), fits
+// [k np 10, (k + 1) np 10) belong to round k.  Records (prepass rule) land in
+// rec, np per round.
+int prepass_rounds(ps_ctx* c, const std::vector<double>& cw, int np, std::vector<ps_record>& rec) {
+    const Problem& p = c->prob;
+    const int R = (int)cw.size(), rows_n = 4 * (p.n_points + 3);
+    std::vector<double> rows((size_t)R * rows_n);
+    std::vector<psb::DevProblem> dps(R, c->dp);
+    PSB_CUDA(c->d_pre_rows.ensure(rows.size()));
+    for (int k = 0; k < R; k++) {
+        build_rows(p, cw[k], rows.data() + (size_t)k * rows_n);
+        const double* base = c->d_pre_rows.p + (size_t)k * rows_n;
+        const int nr = p.n_points + 3;
+        dps[k].yobs = base;
+        dps[k].sig = base + nr;
+        dps[k].sig2i = base + 2 * nr;
+        dps[k].wght = base + 3 * nr;
+        dps[k].conw_r = cw[k];
+    }
+    std::vector<int> ctl(2 * R + 1);
+    for (int k = 0; k <= R; k++) ctl[k] = k * np * 10;
+    for (int k = 0; k < R; k++) ctl[R + 1 + k] = 1;
+    PSB_CUDA(c->d_pre_rows.upload(rows, c->stream));
+    PSB_CUDA(c->d_pre_dp.upload(dps, c->stream));
+    PSB_CUDA(c->d_pre_ctl.upload(ctl, c->stream));
+    const int n_fits = R * np * 10;
+    PSB_CUDA(c->d_fits.ensure(n_fits));
+    int grid = c->sms * c->blocks_per_sm;
+    if (grid > n_fits) grid = n_fits;
+    int rc = ensure_scratch(c, grid);
+    if (rc) return rc;
+    PSB_CUDA(cudaMemsetAsync(c->d_queue.p, 0, sizeof(int), c->stream));
+    psb::FitBatch b{};
+    b.n_from = 1;
+    b.n_fits = n_fits;
+    b.queue = c->d_queue.p;
+    b.out = c->d_fits.p;
+    b.scratch = c->d_scratch.p;
+    b.scratch_stride = (long long)scratch_stride(c);
+    b.n_ast = R;
+    b.ast_fit_off = c->d_pre_ctl.p;
+    b.ast_n_from = c->d_pre_ctl.p + R + 1;
+    if (c->form == PS_FORM_FAST)
+        PSB_CUDA(psb::launch_fast_fits(c->dp, c->d_pre_dp.p, b, grid, c->stream));
+    else
+        PSB_CUDA(psb::launch_fp64_fits(c->dp, c->d_pre_dp.p, b, grid, c->stream));
+    g_launches++;
+    PSB_CUDA(c->d_rec.ensure((size_t)R * np));
+    PSB_CUDA(psb::launch_period_reduce(c->d_fits.p, R * np, c->dp.ndata_m3, 1, c->d_rec.p, c->stream));
+    g_launches++;
+    rec.resize((size_t)R * np);
+    PSB_CUDA(cudaMemcpyAsync(rec.data(), c->d_rec.p, sizeof(ps_record) * R * np, cudaMemcpyDeviceToHost, c->stream));
+    PSB_CUDA(cudaStreamSynchronize(c->stream));
+    return PS_OK;
+}
+
 int ps_precalc(ps_ctx* c, double* conw_r) {
     int rc = check_ready(c, false);
     if (rc) return rc;
@@ -627,7 +691,35 @@ int ps_precalc(ps_ctx* c, double* conw_r) {
     int new_conw = 0;
     c->prepass_fits = 0;
     std::vector<ps_record> rec(10);
-    // period_search_BOINC.cpp:488-715
+    // period_search_BOINC.cpp:488-715.  The FP64 forms run the rounds the
+    // loop may still need together: round k (convexity weight conw_r 2^k,
+    // while conw_r 2^k escl^2 < 10) has the fits it would have on its own,
+    // so the first round whose mean dark-facet percentage is below 1 %, and
+    // with it conw_r, is the one the sequential loop stops at.
+    if (p.n_periods() < 1) return fail(PS_ERR_LIMIT, "the period range holds no trial period");
+    if (c->form == PS_FORM_FAST || c->form == PS_FORM_FP64) {
+        const int np = std::min(10, p.n_periods());
+        while (!new_conw && p.conw_r * p.escl * p.escl < 10.0) {
+            std::vector<double> cw;
+            for (double w = p.conw_r; (int)cw.size() < 8 && w * p.escl * p.escl < 10.0; w = w * 2) cw.push_back(w);
+            rc = prepass_rounds(c, cw, np, rec);
+            if (rc) return rc;
+            for (int k = 0; k < (int)cw.size() && !new_conw; k++) {
+                c->prepass_fits += 10 * np;
+                double sum_dark_facet = 0.0;
+                for (int n = 0; n < np; n++) sum_dark_facet = sum_dark_facet + rec[(size_t)k * np + n].dark_pct;
+                const double ave_dark_facet = sum_dark_facet / np;
+                if (ave_dark_facet < 1.0)
+                    new_conw = 1;
+                else
+                    p.conw_r = p.conw_r * 2;
+            }
+        }
+        rc = upload_rows(c);
+        if (rc) return rc;
+        if (conw_r) *conw_r = p.conw_r;
+        return PS_OK;
+    }
     while ((new_conw != 1) && ((p.conw_r * p.escl * p.escl) < 10.0)) {
         rc = upload_rows(c);
         if (rc) return rc;

@@ -95,6 +95,10 @@ struct ps_ctx {
     psb::DevBuf<float> d_fac32;
     psb::DevBuf<uint16_t> d_bsw;
     psb::DevBuf<int> d_err;
+    // speculative convexity pre-pass rounds: rows and problem copies per round
+    psb::DevBuf<double> d_pre_rows;
+    psb::DevBuf<psb::DevProblem> d_pre_dp;
+    psb::DevBuf<int> d_pre_ctl;
     std::vector<int> free_idx;
 };
 
