@@ -42,7 +42,11 @@ Inputs:
             inputs are regenerated by periodsearch_b200.synth at test time
             and checked against the sha256 stored in meta.json
 
-Not in the default set (minutes of CPU each): c2, c4_shaped, c5.
+  real      the first 20 trial periods (pre-pass included) of six of the
+            reference's 100 real inputs (period_search/input_period_search),
+            from the reference application and its perturbed builds
+
+Not in the default set (minutes of CPU each): real, c2, c4_shaped, c5.
 """
 from __future__ import annotations
 
@@ -393,6 +397,28 @@ def make_c5(workers):
     print("c5 written", flush=True)
 
 
+REAL_PERIODS = 20  # trial periods of each real-data slice (the pre-pass reads the first ten)
+
+
+def real_inputs():
+    """Six of the reference's 100 real inputs (period_search/input_period_search:
+    survey photometry, lmax = mmax = 3, nrows = 6), spread over their sizes."""
+    d = os.path.join(REF_ROOT, "period_search", "input_period_search")
+    files = sorted(os.listdir(d), key=lambda f: (os.path.getsize(os.path.join(d, f)), f))
+    pick = [files[i] for i in (0, 20, 40, 60, 80, len(files) - 1)]
+    return [(f.split("_")[-1], open(os.path.join(d, f)).read()) for f in pick]
+
+
+def make_real(workers):
+    """The first REAL_PERIODS trial periods of each real input, pre-pass
+    included, from the reference application, its FMA build and the
+    restatement's perturbed builds."""
+    for ident, text in real_inputs():
+        name = "real_" + ident
+        make_workload(name, _slice_text(text, REAL_PERIODS), REAL_PERIODS, min(workers, 4))
+        make_variants(name, min(workers, 4))
+
+
 def main(names):
     from periodsearch_b200 import synth
 
@@ -428,6 +454,8 @@ def main(names):
     for name in ("tiny", "tiny_rel", "c1", "shipped", "tiny_conv", "c1_conv"):
         if name in names or "variants" in names:
             make_variants(name, workers)
+    if "real" in names:
+        make_real(workers)
     if "c2" in names:
         make_c2_spread(workers)
     if "c4_shaped" in names:

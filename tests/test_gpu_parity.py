@@ -175,8 +175,12 @@ def check_records(gpu, ref, spread, label, perturbed=()):
     return int(chaotic.sum()), float(err.max())
 
 
+# the reference's own real inputs (survey photometry), first periods each
+REAL = sorted(d for d in os.listdir(GOLDEN) if d.startswith("real_")) if os.path.isdir(GOLDEN) else []
+
+
 @pytest.mark.parametrize("form", FORMS)
-@pytest.mark.parametrize("name", ["tiny", "tiny_rel", "c1", "shipped", "tiny_conv", "c1_conv"])
+@pytest.mark.parametrize("name", ["tiny", "tiny_rel", "c1", "shipped", "tiny_conv", "c1_conv"] + REAL)
 def test_scan_matches_reference(native, oracle_lib, name, form):
     ref_full = os.path.join(GOLDEN, name, "ref_out.full")
     if not os.path.exists(ref_full):
