@@ -409,14 +409,23 @@ def real_inputs():
     return [(f.split("_")[-1], open(os.path.join(d, f)).read()) for f in pick]
 
 
+def _make_real_one(ident, text):
+    name = "real_" + ident
+    # one slice: the pre-pass must see the first ten periods, as a scan of
+    # the whole 20-period input does (a slice ending before period ten would
+    # run it on fewer)
+    make_workload(name, _slice_text(text, REAL_PERIODS), REAL_PERIODS, 1)
+    make_variants(name, 1)
+    return name
+
+
 def make_real(workers):
     """The first REAL_PERIODS trial periods of each real input, pre-pass
     included, from the reference application, its FMA build and the
-    restatement's perturbed builds."""
-    for ident, text in real_inputs():
-        name = "real_" + ident
-        make_workload(name, _slice_text(text, REAL_PERIODS), REAL_PERIODS, min(workers, 4))
-        make_variants(name, min(workers, 4))
+    restatement's perturbed builds; the inputs in parallel."""
+    todo = real_inputs()
+    with cf.ProcessPoolExecutor(max_workers=min(workers, len(todo))) as ex:
+        list(ex.map(_make_real_one, [i for i, _ in todo], [t for _, t in todo]))
 
 
 def main(names):
