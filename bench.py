@@ -321,7 +321,7 @@ def c4_measure(args, local):
     with mp.get_context("spawn").Pool(min(os.cpu_count() or 1, 16)) as pool:
         made = pool.map(_c4_worker, [(i, workdir) for i in range(args.asteroids)])
     torch.cuda.set_device(local)
-    form = {"fp64": ps.PS_FORM_FP64, "fast": ps.PS_FORM_FAST}[args.form]
+    form = {"fp64": ps.PS_FORM_FP64, "fast": ps.PS_FORM_FAST, "mixed": ps.PS_FORM_MIXED}[args.form]
     # per-asteroid host setup + uploads: on host threads (the product's
     # open_many), timed; one asteroid on one thread for comparison
     t0 = time.perf_counter()
@@ -333,7 +333,7 @@ def c4_measure(args, local):
     P = args.c4_periods
     n_per = np.array([c.n_periods for c in ctxs])
     tiles = None
-    if not args.no_autotune:
+    if not args.no_autotune and args.form != "mixed":  # the mixed form has fixed tiles
         a0 = np.ones(len(ctxs), dtype=np.int32)
         tiles, _ = ps.PeriodSearchBatch.autotune(ctxs, a0, np.minimum(a0 + P - 1, n_per).astype(np.int32))
     batch = ps.PeriodSearchBatch(ctxs)
@@ -571,8 +571,8 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.config == "c4" and args.impl == "b200":
-        if args.form == "mixed":
-            ap.error("the batched form runs the FP64 forms")
+        if args.form == "adjoint":
+            ap.error("the batched scan runs the fp64, fast and mixed forms")
         run_c4(args, local)
         return
     workdir = tempfile.mkdtemp(prefix="psbench")

@@ -169,10 +169,11 @@ int ps_scan_device_noalloc(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, 
  * CUDA graph.  The reference runs one asteroid per process and, in its CUDA
  * port, one thread block per trial period of that asteroid
  * (period_search_cuda/period_search/start_CUDA.cu:654-776); a batch spans
- * asteroids.  The contexts must share the device, the form (PS_FORM_FP64 or
- * PS_FORM_FAST) and lmax, mmax, nrows, and have conw_r settled
- * (ps_precalc / ps_set_conw_r).  The batch borrows the contexts' tables:
- * close the batch before its contexts. */
+ * asteroids.  The contexts must share the device, the form and lmax, mmax,
+ * nrows, and have conw_r settled (ps_precalc / ps_set_conw_r).  The batch
+ * borrows the contexts' tables: close the batch before its contexts.  In
+ * the mixed form ps_batch_scan reports a bounded device wait that gave up
+ * as PS_ERR_DEVICE_LOOP (the fits it ended carry status -1). */
 typedef struct ps_batch ps_batch;
 int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out);
 /* Scan periods n_from[a]..n_to[a] of every asteroid a; records are

@@ -1,5 +1,5 @@
 // Batched scans: many asteroids, uneven point counts and per-fit LM
-// convergence, in one persistent launch (the FP64 forms).
+// convergence, in one persistent launch (any of the three forms).
 //
 // A batch holds the device copies of its contexts' problem descriptors (the
 // per-asteroid tables stay where each context uploaded them), one control
@@ -62,7 +62,32 @@ int ctl_ord_off(int n) { return 5 + 4 * n; }
     } while (0)
 
 size_t smem_of(const ps_batch* b, const psb::DevProblem& p) {
+    if (b->form == PS_FORM_MIXED) return psb::mixed_smem_bytes(p);
     return b->form == PS_FORM_FAST ? psb::fast_smem_bytes(p) : psb::fp64_smem_bytes(p);
+}
+
+cudaError_t launch_fits(const ps_batch* b, const psb::FitBatch& fb) {
+    if (b->form == PS_FORM_MIXED) return psb::launch_mixed_fits(b->head, b->d_probs.p, fb, b->grid, b->stream);
+    if (b->form == PS_FORM_FAST) return psb::launch_fast_fits(b->head, b->d_probs.p, fb, b->grid, b->stream);
+    return psb::launch_fp64_fits(b->head, b->d_probs.p, fb, b->grid, b->stream);
+}
+
+// The mixed form's bounded device waits report through each context's
+// error flag (fits they ended carry status -1); read after a synchronisation.
+int check_device_errors(ps_batch* b) {
+    if (b->form != PS_FORM_MIXED) return PS_OK;
+    for (int a = 0; a < b->n; a++) {
+        const ps_ctx* c = b->ctx[a];
+        if (!c->d_err.p) continue;
+        int e = 0;
+        PSB_BCUDA(cudaMemcpy(&e, c->d_err.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) {
+            PSB_BCUDA(cudaMemset(c->d_err.p, 0, sizeof(int)));
+            return psb::set_error(PS_ERR_DEVICE_LOOP, "a device wait on the tensor-core pipeline gave up (" +
+                                                          std::to_string(e) + "); the fits it ended carry status -1");
+        }
+    }
+    return PS_OK;
 }
 
 void release_graph(ps_batch* b) {
@@ -92,9 +117,7 @@ int capture(ps_batch* b, size_t fits, size_t periods) {
     fb.ast_ord_off = ctl + ctl_ord_off(b->n);
     PSB_BCUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
     cudaError_t e = cudaMemcpyAsync(ctl, b->h_ctl, b->ctl_ints * sizeof(int), cudaMemcpyHostToDevice, b->stream);
-    if (e == cudaSuccess)
-        e = b->form == PS_FORM_FAST ? psb::launch_fast_fits(b->head, b->d_probs.p, fb, b->grid, b->stream)
-                                    : psb::launch_fp64_fits(b->head, b->d_probs.p, fb, b->grid, b->stream);
+    if (e == cudaSuccess) e = launch_fits(b, fb);
     if (e == cudaSuccess)
         e = psb::launch_period_reduce_batch(b->d_fits.p, ctl + 1, (int)periods, b->n, ctl + ctl_per_off(b->n),
                                             b->d_ndata.p, b->d_rec.p, b->stream);
@@ -182,7 +205,6 @@ int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out) {
         if (!c || c->host_only) why = "context without a device";
         else if (c->device != c0->device) why = "contexts on different devices";
         else if (c->form != c0->form) why = "contexts of different forms";
-        else if (c->form != PS_FORM_FP64 && c->form != PS_FORM_FAST) why = "batches run the FP64 forms";
         else if (!c->rows_ready) why = "call ps_precalc or ps_set_conw_r on every context first";
         else if (c->dp.NCB != c0->dp.NCB || c->dp.F != c0->dp.F || c->dp.C != c0->dp.C || c->dp.ma != c0->dp.ma)
             why = "all asteroids of a batch need the same lmax, mmax and nrows";
@@ -220,7 +242,8 @@ int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out) {
         }
         if (probs[a].dsph == ctxs[a]->dp.dsph) owners.push_back(a);
         ndata[a] = ctxs[a]->dp.ndata_m3;
-        b->stride = std::max(b->stride, (long long)(ctxs[a]->dp.ma + 1) * ctxs[a]->dp.npad);
+        b->stride = std::max(b->stride, b->form == PS_FORM_MIXED ? psb::mixed_scratch_doubles(ctxs[a]->dp)
+                                                                 : (long long)(ctxs[a]->dp.ma + 1) * ctxs[a]->dp.npad);
         const size_t s = smem_of(b, probs[a]);
         if (s >= best) {
             best = s;
@@ -228,8 +251,9 @@ int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out) {
         }
     }
     int threads = 0, sms = 0;
-    const int per_sm = b->form == PS_FORM_FAST ? psb::fast_max_blocks_per_sm(b->head, &threads)
-                                               : psb::fp64_max_blocks_per_sm(b->head, &threads);
+    const int per_sm = b->form == PS_FORM_MIXED  ? psb::mixed_max_blocks_per_sm(b->head, &threads)
+                       : b->form == PS_FORM_FAST ? psb::fast_max_blocks_per_sm(b->head, &threads)
+                                                 : psb::fp64_max_blocks_per_sm(b->head, &threads);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     b->grid = sms * per_sm;
     b->ctl_ints = (size_t)(6 + 5 * n);
@@ -267,7 +291,7 @@ int ps_batch_scan(ps_batch* b, const int* n_from, const int* n_to, ps_record* ou
     if (rc) return rc;
     PSB_BCUDA(cudaMemcpyAsync(out, b->d_rec.p, periods * sizeof(ps_record), cudaMemcpyDeviceToHost, b->stream));
     PSB_BCUDA(cudaStreamSynchronize(b->stream));
-    return PS_OK;
+    return check_device_errors(b);
 }
 
 int ps_batch_fit_times(ps_batch* b, double* busy_ms, double* done_ms) {

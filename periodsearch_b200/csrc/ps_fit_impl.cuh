@@ -606,7 +606,8 @@ __device__ __forceinline__ void eval_scalars(const double* a, int C, double* B, 
 
 // curv.c:15-37: g = exp(sum over (m, l) of Pleg * (c*Fc + s*Fs)), thread per
 // facet; area = Darea g, zero for the 128 slots past F.
-__device__ __forceinline__ void curv_phase(const DevProblem& P, const double* a, double* g, double* area) {
+__device__ __forceinline__ void curv_phase(const DevProblem& P, const double* a, double* g, double* area,
+                                           bool pad = true) {
     const int F = P.F;
     for (int f = threadIdx.x; f < F; f += kThreads) {
         const double* pl = P.cpl + (size_t)f * P.nq;
@@ -631,7 +632,8 @@ __device__ __forceinline__ void curv_phase(const DevProblem& P, const double* a,
         g[f] = gi;
         area[f] = P.fac[(size_t)f * 4 + 3] * gi;
     }
-    for (int f = F + threadIdx.x; f < F + 128; f += kThreads) area[f] = 0.0;
+    if (pad)
+        for (int f = F + threadIdx.x; f < F + 128; f += kThreads) area[f] = 0.0;
 }
 
 // chi2 over all rows (mrqcof.c:119-135) from the normalised model yt.  The
@@ -664,32 +666,27 @@ __device__ __forceinline__ void chi2_rows(const DevProblem& P, const double* yt,
     }
 }
 
-// The model alone at parameters a (sm offset a_off): what the LM step's
-// accept/reject test and the stop rule read from mrqcof at a trial point --
-// chi2, the convexity residuals chck (conv.c:22-27) and the facet-area sum --
-// without the Jacobian or alpha/beta.  curv, the brightness of every point
+// The model alone at parameters a: what the LM step's accept/reject test and
+// the stop rule read from mrqcof at a trial point -- chi2, the convexity
+// residuals chck (conv.c:22-27) and the facet-area sum -- without the
+// Jacobian or alpha/beta.  curv, the brightness of every point
 // (bright.c:54-76, 106-125 without the derivative terms), the convexity
 // rows, the relative-lightcurve normalisation of the model (mrqcof.c:53-58,
 // 92-104) and chi2, with the operations and sum orders of evaluate(), so
 // that in the reference-order form every value is bit-identical to the one
 // evaluate() gives at the same point.  The model goes to yt; Jt is not
 // touched.  Thread per data point, facet normals staged in chunks of kMf.
-template <int NCB, bool kFast>
-__device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, int a_off, double* yt) {
-    extern __shared__ __align__(16) double sm[];
-    const double* a = sm + a_off;
-    const DevProblem& P = *Pp;
-    const Layout L = make_layout(P);
+// Buffers (shared memory): g, area [F] (area is not padded past F here);
+// misc and B/D (blmatrix) as in evaluate(); work >= max(sortseg, 4 kMf,
+// kThreads) doubles, 16-byte aligned; perm sortseg ints.  Used by the FP64
+// fit kernels (evaluate_model) and the mixed-precision one.
+template <bool kFast>
+__device__ void model_pass(const DevProblem& P, const double* a, double* g, double* area, double* misc, double* B,
+                           double* D, double* work, int* perm, double* yt) {
     const int tid = threadIdx.x;
     const int F = P.F, C = P.C;
-    double* g = sm + L.g;
-    double* area = sm + L.area;
-    double* misc = sm + L.misc;
-    double* B = sm + L.blm;
-    double* D = sm + L.blm + 9;
-    double* work = sm + L.work;
     eval_scalars(a, C, B, D, misc);
-    curv_phase(P, a, g, area);
+    curv_phase(P, a, g, area, false);
     __syncthreads();
     // chck and the facet-area sum, facets in order (as evaluate() and the
     // fast point loop form them); four threads, loads ahead of the sums
@@ -706,7 +703,6 @@ __device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, i
         }
     }
     const double cl = misc[M_CL], cls = misc[M_CLS];
-    int* perm = (int*)(sm + L.perm);
     // points in segments sorted by viewing direction (as in evaluate()), so
     // that the points of a warp see nearly the same facets
     for (int s0 = 0; s0 < P.n_points; s0 += P.sortseg) {
@@ -802,6 +798,15 @@ __device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, i
     __syncthreads();
     chi2_rows<kFast>(P, yt, misc);
     __syncthreads();
+}
+
+template <int NCB, bool kFast>
+__device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, int a_off, double* yt) {
+    extern __shared__ __align__(16) double sm[];
+    const DevProblem& P = *Pp;
+    const Layout L = make_layout(P);
+    model_pass<kFast>(P, sm + a_off, sm + L.g, sm + L.area, sm + L.misc, sm + L.blm, sm + L.blm + 9, sm + L.work,
+                      (int*)(sm + L.perm), yt);
 }
 
 template <int NCB, bool kFast>

@@ -34,6 +34,7 @@
 
 #include "ps_device.hpp"
 #include "ps_fit_common.cuh"
+#include "ps_fit_impl.cuh"
 #include "ps_umma.cuh"
 
 namespace psb {
@@ -69,6 +70,15 @@ struct MLayout {
     size_t bytes;                                 // total incl. 1024 B alignment slack
 };
 
+// Doubles of the model pass's work buffer (staged normals, sort keys,
+// lightcurve sums).
+__host__ __device__ inline int model_work_doubles(const DevProblem& P) {
+    int w = 4 * fitimpl::kMf;
+    if (P.sortseg > w) w = P.sortseg;
+    if (kThreads > w) w = kThreads;
+    return w;
+}
+
 __host__ __device__ inline MLayout make_mlayout(const DevProblem& P) {
     MLayout L;
     uint32_t o = 0;
@@ -88,6 +98,8 @@ __host__ __device__ inline MLayout make_mlayout(const DevProblem& P) {
     // kRtM x (mfit + 1) + kRtM x mfit floats, well inside 96 KB
     L.mbar = o;
     o += 32;
+    // TMEM base address, then the work item and asteroid of the current fit
+    // (broadcast before the fit's own layout is known)
     L.tslot = o;
     o += 16;
     // per-tile exchange of the second thread's partial sums: 128 x (double + 8 floats)
@@ -541,6 +553,21 @@ __device__ __noinline__ void evaluate_mixed(const DevProblem* __restrict__ Pp, u
     __syncthreads();
 }
 
+// The model alone at a trial point (fitimpl::model_pass: FP64, the fast
+// form's arithmetic), with the operand-tile region -- idle between
+// evaluations -- as its g, work and perm buffers.
+__device__ __noinline__ void evaluate_model_mixed(const DevProblem* __restrict__ Pp, uint8_t* raw, const double* a,
+                                                  double* yt) {
+    const DevProblem& P = *Pp;
+    const MPtr M = mptrs(P, raw);
+    const MLayout& L = M.L;
+    double* g = (double*)M.base;
+    const size_t work_off = (((size_t)P.F * 8) + 255) & ~(size_t)255;
+    double* work = (double*)(M.base + work_off);
+    int* perm = (int*)(M.base + work_off + (size_t)model_work_doubles(P) * 8);
+    fitimpl::model_pass<true>(P, a, g, M.d(L.area), M.d(L.misc), M.d(L.blm), M.d(L.blm) + 9, work, perm, yt);
+}
+
 __device__ void tmem_setup(const DevProblem& P, uint8_t* raw, uint32_t* tmem) {
     const MPtr M = mptrs(P, raw);
     uint32_t* slot = (uint32_t*)(M.base + M.L.tslot);
@@ -572,40 +599,84 @@ __device__ void tmem_teardown(const DevProblem& P, uint8_t* raw, uint32_t tmem) 
     if ((threadIdx.x >> 5) == 0) umma::tmem_dealloc(tmem, kTmemCols);
 }
 
-__global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem* __restrict__ Pp, FitBatch Bt) {
+// Persistent: one fit per CTA at a time from the work queue.  In a batch
+// (Bt.n_ast > 1) the problems Parr[a] share lmax, mmax and nrows and differ
+// in their data and in mfit (calibrated lightcurves free one more
+// parameter), so the shared-memory layout is set per fit (the launch gives
+// the largest); only the byte regions before the doubles (operand tiles,
+// mbarriers, TMEM slot, work slots) are the same for all.  The fits of
+// asteroid a are [ast_fit_off[a], ast_fit_off[a + 1]) of the queue, in queue
+// order ast_order when it is given (largest asteroid first).
+__global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem* __restrict__ Parr, FitBatch Bt) {
     extern __shared__ uint8_t smem_raw[];
-    const DevProblem& P = *Pp;
-    const MPtr M = mptrs(P, smem_raw);
-    const MLayout& L = M.L;
     const int tid = threadIdx.x;
-    const int C = P.C, ma = P.ma, mfit = P.mfit;
-    double* cg = M.d(L.cg);
-    double* atry = M.d(L.atry);
-    double* misc = M.d(L.misc);
-    int* ipiv = M.ints + L.ipiv;
-    entry_map(mfit, M.ints + L.ent);
     uint32_t tmem;
-    tmem_setup(P, smem_raw, &tmem);
+    tmem_setup(Parr[0], smem_raw, &tmem);
+    int* qslot;  // [0] work item, [1] asteroid
+    {
+        const MPtr M0 = mptrs(Parr[0], smem_raw);
+        qslot = (int*)(M0.base + M0.L.tslot) + 1;
+    }
     uint32_t gc = 0;
-    float* Jf = (float*)(Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride);
-    double* yt = Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride + ((size_t)ma * P.npad + 1) / 2;
-    if (tid == 0) misc[M_ABORT] = 0;
+    int cur_mfit = -1;
     bool aborted = false;
 
     while (!aborted) {
         __syncthreads();
-        if (tid == 0) misc[M_WORK] = (double)atomicAdd(Bt.queue, 1);
+        if (tid == 0) {
+            const int nf = Bt.n_fits_dev ? *Bt.n_fits_dev : Bt.n_fits;
+            int w = atomicAdd(Bt.queue, 1);
+            int a = 0;
+            if (w >= nf) {
+                w = -1;
+            } else if (Bt.n_ast > 1) {
+                const int* off = Bt.ast_order ? Bt.ast_ord_off : Bt.ast_fit_off;
+                int lo = 0, hi = Bt.n_ast - 1;  // last k with off[k] <= w
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (off[mid] <= w)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                a = lo;
+                if (Bt.ast_order) {
+                    a = Bt.ast_order[lo];
+                    w = Bt.ast_fit_off[a] + (w - off[lo]);
+                }
+            }
+            qslot[0] = w;
+            qslot[1] = a;
+        }
         __syncthreads();
-        const int w = (int)misc[M_WORK];
-        if (w >= Bt.n_fits) break;
+        const int w = qslot[0];
+        if (w < 0) break;
+        const unsigned long long t_start = fitimpl::global_ns();
+        const int ast = qslot[1];
+        const DevProblem* Pp = Parr + ast;
+        const DevProblem& P = *Pp;
+        const MPtr M = mptrs(P, smem_raw);
+        const MLayout& L = M.L;
+        const int C = P.C, ma = P.ma, mfit = P.mfit;
+        double* cg = M.d(L.cg);
+        double* atry = M.d(L.atry);
+        double* misc = M.d(L.misc);
+        if (mfit != cur_mfit) {
+            entry_map(mfit, M.ints + L.ent);
+            cur_mfit = mfit;
+        }
+        if (tid == 0) misc[M_ABORT] = 0;
+        float* Jf = (float*)(Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride);
+        double* yt = Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride + ((size_t)ma * P.npad + 1) / 2;
         double freq;
         int pole;
         if (Bt.pole_override) {
             freq = Bt.freq_override;
             pole = Bt.pole_override;
         } else {
-            const int n = Bt.n_from + w / 10;
-            pole = w % 10 + 1;
+            const int local = Bt.n_ast > 1 ? w - Bt.ast_fit_off[ast] : w;
+            const int n = (Bt.n_ast > 1 ? Bt.ast_n_from[ast] : Bt.n_from) + local / 10;
+            pole = local % 10 + 1;
             freq = P.freq_start - (n - 1) * P.freq_step;
         }
         for (int i = tid; i < ma; i += kThreads) {
@@ -636,9 +707,13 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
         double* covar = M.d(L.covar);
         double* beta = M.d(L.beta);
         double* da = M.d(L.da);
+        // LM loop as in the FP64 fit kernels: a trial point gets the model
+        // alone (FP64), alpha and beta are evaluated at an accepted point when
+        // the next step needs them.
         double alamda = -1, ochisq = 0, chisq = 0, iter_diff = 1e40, dev_old = 1e30, dev_new = 0, rchisq = -1;
         double chk0 = 0, chk1 = 0, chk2 = 0, cur0 = 0, cur1 = 0, cur2 = 0, s_cur = 0, s_last = 0;
         int niter = 0, status = 0;
+        bool j_stale = false;
         while (((niter < P.n_iter_max) && (iter_diff > P.iter_diff_max)) || (niter < P.n_iter_min)) {
             if (alamda < 0) {
                 alamda = P.alamda_start;
@@ -653,6 +728,13 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
                 cur2 = misc[M_CHK0 + 2];
                 s_cur = s_last = misc[M_SAREA];
                 for (int i = tid; i < ma; i += kThreads) atry[i] = cg[i];
+            } else if (j_stale) {
+                evaluate_mixed(Pp, smem_raw, cg, alpha, beta, Jf, yt, tmem, &gc);
+                if (misc[M_ABORT] != 0) {
+                    aborted = true;
+                    break;
+                }
+                j_stale = false;
             }
             for (int idx = tid; idx < mfit * mfit; idx += kThreads) {
                 const int j = idx / mfit, k = idx - j * mfit;
@@ -668,22 +750,13 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
                     atry[l] = cg[l] + da[j];
                 }
                 __syncthreads();
-                evaluate_mixed(Pp, smem_raw, atry, covar, da, Jf, yt, tmem, &gc);
-                if (misc[M_ABORT] != 0) {
-                    aborted = true;
-                    break;
-                }
+                evaluate_model_mixed(Pp, smem_raw, atry, yt);
                 const double temp = misc[M_CHISQ];
                 chisq = temp;
                 s_last = misc[M_SAREA];
                 if (temp < ochisq) {
                     alamda = alamda / P.alamda_incr;
-                    double* t1 = alpha;
-                    alpha = covar;
-                    covar = t1;
-                    t1 = beta;
-                    beta = da;
-                    da = t1;
+                    j_stale = true;
                     for (int i = tid; i < ma; i += kThreads) cg[i] = atry[i];
                     cur0 = misc[M_CHK0];
                     cur1 = misc[M_CHK0 + 1];
@@ -724,12 +797,13 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
             o.chisq = aborted ? __longlong_as_double(0x7ff8000000000000ll) : chisq;
             o.niter = niter;
             o.status = aborted ? -1 : status;
-            o.dur_us = 0;
-            o.end_us = 0;
+            const unsigned long long t_end = fitimpl::global_ns();
+            o.dur_us = (unsigned int)((t_end - t_start) / 1000ull);
+            o.end_us = (unsigned int)(t_end / 1000ull);
             Bt.out[w] = o;
         }
     }
-    tmem_teardown(P, smem_raw, tmem);
+    tmem_teardown(Parr[0], smem_raw, tmem);
 }
 
 __global__ void __launch_bounds__(kThreads, 1) mixed_eval_kernel(const DevProblem* __restrict__ Pp, EvalOut E) {
@@ -761,7 +835,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_eval_kernel(const DevProble
 
 bool mixed_supported(const DevProblem& P) {
     return P.C <= kNc && P.nchunk * kKc >= P.F && P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 <= kMaxEptM * kThreads &&
-           P.mfit <= 0xffff && P.bsw && P.fac32 && P.err;
+           P.mfit <= 0xffff && P.bsw && P.fac32 && P.err &&
+           ((((size_t)P.F * 8) + 255) & ~(size_t)255) + (size_t)model_work_doubles(P) * 8 + (size_t)P.sortseg * 4 <=
+               (size_t)(4 * kTileP * 128 + 4 * kNc * 128);
 }
 
 }  // namespace

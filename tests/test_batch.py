@@ -25,10 +25,10 @@ def _asteroids(tmp_path, n=4):
     return paths
 
 
-@pytest.mark.parametrize("form", ["fp64", "fast"])
+@pytest.mark.parametrize("form", ["fp64", "fast", "mixed"])
 def test_batch_equals_single_scans(native, tmp_path, form):
     ps = native
-    fid = {"fp64": ps.PS_FORM_FP64, "fast": ps.PS_FORM_FAST}[form]
+    fid = {"fp64": ps.PS_FORM_FP64, "fast": ps.PS_FORM_FAST, "mixed": ps.PS_FORM_MIXED}[form]
     ctxs = [ps.PeriodSearch(p, form=fid) for p in _asteroids(tmp_path)]
     for c in ctxs:
         c.set_conw_r(c.conw_r * 4)
