@@ -444,11 +444,11 @@ int run_fits(ps_ctx* c, int n_from, int n_fits, int pole_override, double freq_o
     return PS_OK;
 }
 
-int scan_into(ps_ctx* c, int n_from, int n_to, ps_record* d_out, int prepass) {
+int scan_into(ps_ctx* c, int n_from, int n_to, ps_record* d_out) {
     const int np = n_to - n_from + 1;
     int rc = run_fits(c, n_from, np * 10, 0, 0.0);
     if (rc) return rc;
-    PSB_CUDA(psb::launch_period_reduce(c->d_fits.p, np, c->dp.ndata_m3, prepass, d_out, c->stream));
+    PSB_CUDA(psb::launch_period_reduce(c->d_fits.p, np, c->dp.ndata_m3, 0, d_out, c->stream));
     g_launches++;
     return PS_OK;
 }
@@ -669,7 +669,9 @@ int prepass_rounds(ps_ctx* c, const std::vector<double>& cw, int np, std::vector
     b.n_ast = R;
     b.ast_fit_off = c->d_pre_ctl.p;
     b.ast_n_from = c->d_pre_ctl.p + R + 1;
-    if (c->form == PS_FORM_FAST)
+    if (c->form == PS_FORM_MIXED)
+        PSB_CUDA(psb::launch_mixed_fits(c->dp, c->d_pre_dp.p, b, grid, c->stream));
+    else if (c->form == PS_FORM_FAST)
         PSB_CUDA(psb::launch_fast_fits(c->dp, c->d_pre_dp.p, b, grid, c->stream));
     else
         PSB_CUDA(psb::launch_fp64_fits(c->dp, c->d_pre_dp.p, b, grid, c->stream));
@@ -680,7 +682,7 @@ int prepass_rounds(ps_ctx* c, const std::vector<double>& cw, int np, std::vector
     rec.resize((size_t)R * np);
     PSB_CUDA(cudaMemcpyAsync(rec.data(), c->d_rec.p, sizeof(ps_record) * R * np, cudaMemcpyDeviceToHost, c->stream));
     PSB_CUDA(cudaStreamSynchronize(c->stream));
-    return PS_OK;
+    return check_device_error(c);
 }
 
 int ps_precalc(ps_ctx* c, double* conw_r) {
@@ -691,55 +693,28 @@ int ps_precalc(ps_ctx* c, double* conw_r) {
     int new_conw = 0;
     c->prepass_fits = 0;
     std::vector<ps_record> rec(10);
-    // period_search_BOINC.cpp:488-715.  The FP64 forms run the rounds the
-    // loop may still need together: round k (convexity weight conw_r 2^k,
-    // while conw_r 2^k escl^2 < 10) has the fits it would have on its own,
-    // so the first round whose mean dark-facet percentage is below 1 %, and
-    // with it conw_r, is the one the sequential loop stops at.
+    // period_search_BOINC.cpp:488-715, with the rounds the loop may still
+    // need run together: round k (convexity weight conw_r 2^k, while
+    // conw_r 2^k escl^2 < 10) has the fits it would have on its own, so the
+    // first round whose mean dark-facet percentage is below 1 %, and with it
+    // conw_r, is the one the sequential loop stops at.
     if (p.n_periods() < 1) return fail(PS_ERR_LIMIT, "the period range holds no trial period");
-    if (c->form == PS_FORM_FAST || c->form == PS_FORM_FP64) {
-        const int np = std::min(10, p.n_periods());
-        while (!new_conw && p.conw_r * p.escl * p.escl < 10.0) {
-            std::vector<double> cw;
-            for (double w = p.conw_r; (int)cw.size() < 8 && w * p.escl * p.escl < 10.0; w = w * 2) cw.push_back(w);
-            rc = prepass_rounds(c, cw, np, rec);
-            if (rc) return rc;
-            for (int k = 0; k < (int)cw.size() && !new_conw; k++) {
-                c->prepass_fits += 10 * np;
-                double sum_dark_facet = 0.0;
-                for (int n = 0; n < np; n++) sum_dark_facet = sum_dark_facet + rec[(size_t)k * np + n].dark_pct;
-                const double ave_dark_facet = sum_dark_facet / np;
-                if (ave_dark_facet < 1.0)
-                    new_conw = 1;
-                else
-                    p.conw_r = p.conw_r * 2;
-            }
+    const int np = std::min(10, p.n_periods());
+    while (!new_conw && p.conw_r * p.escl * p.escl < 10.0) {
+        std::vector<double> cw;
+        for (double w = p.conw_r; (int)cw.size() < 8 && w * p.escl * p.escl < 10.0; w = w * 2) cw.push_back(w);
+        rc = prepass_rounds(c, cw, np, rec);
+        if (rc) return rc;
+        for (int k = 0; k < (int)cw.size() && !new_conw; k++) {
+            c->prepass_fits += 10 * np;
+            double sum_dark_facet = 0.0;
+            for (int n = 0; n < np; n++) sum_dark_facet = sum_dark_facet + rec[(size_t)k * np + n].dark_pct;
+            const double ave_dark_facet = sum_dark_facet / np;
+            if (ave_dark_facet < 1.0)
+                new_conw = 1;
+            else
+                p.conw_r = p.conw_r * 2;
         }
-        rc = upload_rows(c);
-        if (rc) return rc;
-        if (conw_r) *conw_r = p.conw_r;
-        return PS_OK;
-    }
-    while ((new_conw != 1) && ((p.conw_r * p.escl * p.escl) < 10.0)) {
-        rc = upload_rows(c);
-        if (rc) return rc;
-        int max_test_periods = 10;
-        double sum_dark_facet = 0.0;
-        const int n_iter = p.n_periods();
-        if (n_iter < max_test_periods) max_test_periods = n_iter;
-        PSB_CUDA(c->d_rec.ensure(10));
-        rc = scan_into(c, 1, max_test_periods, c->d_rec.p, 1);
-        if (rc) return rc;
-        c->prepass_fits += 10 * max_test_periods;
-        PSB_CUDA(cudaMemcpyAsync(rec.data(), c->d_rec.p, sizeof(ps_record) * max_test_periods,
-                                 cudaMemcpyDeviceToHost, c->stream));
-        PSB_CUDA(cudaStreamSynchronize(c->stream));
-        rc = check_device_error(c);
-        if (rc) return rc;
-        for (int n = 0; n < max_test_periods; n++) sum_dark_facet = sum_dark_facet + rec[n].dark_pct;
-        const double ave_dark_facet = sum_dark_facet / max_test_periods;
-        if (ave_dark_facet < 1.0) new_conw = 1;
-        if (ave_dark_facet >= 1.0) p.conw_r = p.conw_r * 2;
     }
     rc = upload_rows(c);
     if (rc) return rc;
@@ -799,7 +774,7 @@ int ps_autotune(ps_ctx* c, int n_periods, int* tiles, double* seconds) {
     auto timed = [&](double& t) -> int {
         PSB_CUDA(cudaStreamSynchronize(c->stream));
         const auto t0 = std::chrono::steady_clock::now();
-        int r = scan_into(c, 1, np, c->d_rec.p, 0);
+        int r = scan_into(c, 1, np, c->d_rec.p);
         if (r) return r;
         PSB_CUDA(cudaStreamSynchronize(c->stream));
         t = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -847,7 +822,7 @@ int ps_scan_device(ps_ctx* c, int n_from, int n_to, ps_record* d_out, void* stre
     PSB_CUDA(cudaSetDevice(c->device));
     cudaStream_t saved = c->stream;
     if (stream) c->stream = (cudaStream_t)stream;
-    rc = scan_into(c, n_from, n_to, d_out, 0);
+    rc = scan_into(c, n_from, n_to, d_out);
     c->stream = saved;
     if (rc) return rc;
     if (stream) PSB_CUDA(psb::note_caller_stream(c, (cudaStream_t)stream));
@@ -862,7 +837,7 @@ int ps_scan(ps_ctx* c, int n_from, int n_to, ps_record* out) {
     PSB_CUDA(cudaSetDevice(c->device));
     const int np = n_to - n_from + 1;
     PSB_CUDA(c->d_rec.ensure(np));
-    rc = scan_into(c, n_from, n_to, c->d_rec.p, 0);
+    rc = scan_into(c, n_from, n_to, c->d_rec.p);
     if (rc) return rc;
     PSB_CUDA(cudaMemcpyAsync(out, c->d_rec.p, sizeof(ps_record) * np, cudaMemcpyDeviceToHost, c->stream));
     PSB_CUDA(cudaStreamSynchronize(c->stream));

@@ -109,6 +109,18 @@ try:
 except ps.PeriodSearchError as e:
     print("CODE", e.code)
 g.close()
+cs = [ps.PeriodSearch(sys.argv[2], form=ps.PS_FORM_MIXED) for _ in range(2)]
+for c in cs:
+    c.set_conw_r(c.conw_r)
+b = ps.PeriodSearchBatch(cs)
+try:
+    b.scan([1, 1], [2, 3])
+    print("BATCH_NO_ERROR")
+except ps.PeriodSearchError as e:
+    print("BATCH_CODE", e.code)
+b.close()
+for c in cs:
+    c.close()
 h = ps.PeriodSearch(sys.argv[2], form=ps.PS_FORM_FP64)
 h.set_conw_r(h.conw_r)
 rec = h.scan(1, 3)
@@ -120,8 +132,9 @@ def test_bounded_wait_gives_up_and_reports(native, tmp_path):
     """The tensor-core waits of the mixed kernel are bounded.  With the limit
     set to zero polls (PS_B200_MAX_POLLS=0) every such wait gives up at
     once: the kernel drains its own MMAs, frees its TMEM and returns, the scan
-    reports PS_ERR_DEVICE_LOOP, and the GPU context stays usable (an FP64
-    scan in the same process afterwards succeeds)."""
+    reports PS_ERR_DEVICE_LOOP (a single scan and a batched one), and the
+    GPU context stays usable (an FP64 scan in the same process afterwards
+    succeeds)."""
     import subprocess
     import sys
 
@@ -133,5 +146,6 @@ def test_bounded_wait_gives_up_and_reports(native, tmp_path):
     r = subprocess.run([sys.executable, str(script), REPO, golden_path("tiny")], env=env, capture_output=True,
                        text=True, timeout=300)
     assert r.returncode == 0, r.stderr
-    assert "CODE %d" % native.PS_ERR_DEVICE_LOOP in r.stdout, r.stdout
+    assert "\nCODE %d" % native.PS_ERR_DEVICE_LOOP in "\n" + r.stdout, r.stdout
+    assert "BATCH_CODE %d" % native.PS_ERR_DEVICE_LOOP in r.stdout, r.stdout
     assert "AFTER 1" in r.stdout, r.stdout
