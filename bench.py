@@ -534,6 +534,15 @@ def run_adjoint(args, path, local):
             "gpu_launches": int(launches), "clocks": clk.summary(),
             "e2e": {"value": rate, "unit": "products/s", "h2d_bytes_per_step": int(n * 8 * (g.ma + g.ma)),
                     "d2h_bytes_per_step": int(n * 8 * (g.mfit + 1))}}
+    if not args.profile:
+        # one whole LM fit driven by these kernels alone (ps_fit_jfree)
+        t0 = time.perf_counter()
+        rj = g.fit_jfree(g.freq_start, 1)
+        tj = time.perf_counter() - t0
+        line["jfree_fit"] = {"fits_per_s": 1.0 / tj, "seconds": tj, "niter": int(rj["niter"]),
+                             "what": "one Jacobian-free LM fit (ps_fit_jfree, period 1, pole 1): per accepted step "
+                                     "alpha from mfit Gauss-Newton products plus the gradient pass, per trial "
+                                     "point the gradient pass, each over the whole GPU; the solve on the host"}
     g.close()
     print(json.dumps(line), flush=True)
 

@@ -254,6 +254,16 @@ int ps_autotune(ps_ctx* ctx, int n_periods, int* tiles, double* seconds);
  * counterpart in the reference (it forms alpha explicitly). */
 int ps_chi2_grad(ps_ctx* ctx, const double* a, double* chi2, double* beta);
 int ps_gn_product(ps_ctx* ctx, const double* a, const double* v, double* out);
+/* One LM fit as ps_fit (period_search_BOINC.cpp:817-920; mrqmin.c:11-110
+ * with gauss_errc's full pivoting), Jacobian-free: every model evaluation
+ * runs the matrix-free kernels, alpha column by column from mfit
+ * Gauss-Newton products with the free unit vectors, beta and chi2 from the
+ * gradient pass, the trial points from the gradient pass alone, and the
+ * solve on the host in FP64.  J is never formed (for shapes whose N x ma
+ * Jacobian would not fit); each accepted step costs mfit + 1 matrix-free
+ * passes over the whole GPU, so for shapes whose J fits, ps_fit and the
+ * scans are far faster.  Same outputs as ps_fit, up to rounding. */
+int ps_fit_jfree(ps_ctx* ctx, double freq, int pole, ps_fit_result* out, double* cg_out);
 
 /* Message for the last error on the calling thread ("" if none). */
 const char* ps_last_error(void);

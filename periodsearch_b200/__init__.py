@@ -116,7 +116,7 @@ EXPORTS = (
     "ps_scan_device", "ps_fit", "ps_mrqcof", "ps_model", "ps_info", "ps_get_array", "ps_open_host_only",
     "ps_format_record", "ps_last_error", "ps_kernel_launches", "ps_scan_device_noalloc",
     "ps_batch_open", "ps_batch_scan", "ps_batch_scan_device", "ps_batch_fit_times", "ps_batch_close",
-    "ps_fp64_tensor_peak", "ps_chi2_grad", "ps_gn_product", "ps_set_tiles", "ps_autotune",
+    "ps_fp64_tensor_peak", "ps_chi2_grad", "ps_gn_product", "ps_fit_jfree", "ps_set_tiles", "ps_autotune",
     "ps_release_cached_memory",
 )
 
@@ -160,6 +160,7 @@ def load_library(path: str | None = None):
         "ps_set_tiles": (ctypes.c_int, [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
         "ps_autotune": (ctypes.c_int, [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _D]),
         "ps_gn_product": (ctypes.c_int, [vp, _D, _D, _D]),
+        "ps_fit_jfree": (ctypes.c_int, [vp, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_FitResult), _D]),
         "ps_release_cached_memory": (None, []),
     }
     for name, (res, args) in sig.items():
@@ -244,10 +245,20 @@ class PeriodSearch:
         _check(self._lib.ps_scan_device(self._h, n_from, n_to, ctypes.c_void_p(d_out_ptr),
                                         ctypes.c_void_p(stream_ptr or None)))
 
-    def fit(self, freq: float, pole: int) -> np.ndarray:
+    def fit(self, freq: float, pole: int, params: bool = False):
+        """One LM fit (ps_fit); with params=True also its final parameters."""
+        return self._fit(self._lib.ps_fit, freq, pole, params)
+
+    def fit_jfree(self, freq: float, pole: int, params: bool = False):
+        """The same fit Jacobian-free (ps_fit_jfree: matrix-free kernels)."""
+        return self._fit(self._lib.ps_fit_jfree, freq, pole, params)
+
+    def _fit(self, fn, freq, pole, params):
         r = _FitResult()
-        _check(self._lib.ps_fit(self._h, float(freq), int(pole), ctypes.byref(r), None))
-        return np.array([tuple(getattr(r, n) for n, _ in _FitResult._fields_)], dtype=FIT_DTYPE)[0]
+        cg = np.zeros(self.ma)
+        _check(fn(self._h, float(freq), int(pole), ctypes.byref(r), _dptr(cg) if params else None))
+        rec = np.array([tuple(getattr(r, n) for n, _ in _FitResult._fields_)], dtype=FIT_DTYPE)[0]
+        return (rec, cg) if params else rec
 
     def mrqcof(self, a):
         a = np.ascontiguousarray(a, dtype=np.float64)

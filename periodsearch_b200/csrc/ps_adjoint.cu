@@ -55,9 +55,9 @@ inline int facet_slices(const DevProblem& P) {
     return s;
 }
 
-// misc slots
-enum { X_B = 0, X_D = 9, X_CL = 27, X_CLS = 28, X_OMG = 29, X_P1 = 30, X_P2 = 31, X_P3 = 32, X_CHK = 33,
-       X_N = 40 };
+// misc slots (X_CHK and X_SAREA are read by the host: kAdjMiscChk, kAdjMiscSarea)
+enum { X_B = 0, X_D = 9, X_CL = 27, X_CLS = 28, X_OMG = 29, X_P1 = 30, X_P2 = 31, X_P3 = 32, X_CHK = kAdjMiscChk,
+       X_SAREA = kAdjMiscSarea, X_N = 40 };
 
 __device__ double block_sum(double v, double* red) {
     // fixed-order tree: warp shuffles, then warp 0 over the warp partials
@@ -125,25 +125,30 @@ __global__ void adj_curv(const DevProblem* __restrict__ Pp, AdjWork W) {
 }
 
 // Convexity rows: chck_nc = sum Area n_nc and dres_nc,k = sum Darea g Dsph_k
-// n_nc; one warp per sum (lanes stride the facets, fixed-order shuffle tree).
+// n_nc, and the facet-area sum; one warp per sum (lanes stride the facets,
+// fixed-order shuffle tree).
 __global__ void adj_conv(const DevProblem* __restrict__ Pp, AdjWork W) {
     const DevProblem& P = *Pp;
     const int F = P.F, C = P.C, NCB = P.NCB;
     const int job = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (job >= 3 + 3 * C) return;
+    if (job >= 4 + 3 * C) return;
     double s = 0;
     if (job < 3) {
         for (int f = lane; f < F; f += 32) s = fma(W.area[f], P.fac[(size_t)f * 4 + job], s);
+    } else if (job == 3) {
+        for (int f = lane; f < F; f += 32) s += W.area[f];
     } else {
-        const int nc = (job - 3) / C, k = (job - 3) - nc * C;
+        const int nc = (job - 4) / C, k = (job - 4) - nc * C;
         for (int f = lane; f < F; f += 32) s = fma(W.area[f] * P.dsph[(size_t)f * NCB + k], P.fac[(size_t)f * 4 + nc], s);
     }
     for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     if (lane == 0) {
         if (job < 3)
             W.misc[X_CHK + job] = s;
+        else if (job == 3)
+            W.misc[X_SAREA] = s;
         else
-            W.dres[job - 3] = s;
+            W.dres[job - 4] = s;
     }
 }
 
@@ -447,6 +452,8 @@ __global__ void adj_out(const DevProblem* __restrict__ Pp, AdjWork W) {
 
 }  // namespace
 
+size_t adjoint_misc_offset(const DevProblem& P) { return (size_t)P.F * 7 + 3 * (size_t)P.C; }
+
 size_t adjoint_work_doubles(const DevProblem& P) {
     const size_t N = P.n_points, F = P.F;
     const size_t npb = (N + kPtBlock - 1) / kPtBlock;
@@ -500,7 +507,7 @@ cudaError_t launch_adjoint(const DevProblem& P, const DevProblem* dP, double* wo
     const int nlc = P.n_lc - 1;
     const unsigned fb = (unsigned)((F + 255) / 256);
     adj_curv<<<fb, 256, 0, s>>>(dP, W);
-    adj_conv<<<(unsigned)((3 + 3 * P.C + 7) / 8), 256, 0, s>>>(dP, W);
+    adj_conv<<<(unsigned)((4 + 3 * P.C + 7) / 8), 256, 0, s>>>(dP, W);
     adj_points<<<dim3((unsigned)((N + kPtThreads - 1) / kPtThreads), (unsigned)W.nfs), kPtThreads, 0, s>>>(dP, W);
     adj_points_fin<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(dP, W);
     if (nlc > 0) adj_lc<<<(unsigned)nlc, 256, 0, s>>>(dP, W);

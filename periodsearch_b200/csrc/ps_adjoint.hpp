@@ -31,6 +31,12 @@ struct AdjWork {
 };
 
 size_t adjoint_work_doubles(const DevProblem& P);
+// Scalars of the last evaluation at work + adjoint_misc_offset(P): the
+// convexity residuals chck (3) at kAdjMiscChk, the facet-area sum at
+// kAdjMiscSarea.
+size_t adjoint_misc_offset(const DevProblem& P);
+constexpr int kAdjMiscChk = 33;
+constexpr int kAdjMiscSarea = 36;
 // Kernel launches of one launch_adjoint call.
 constexpr int kAdjointLaunches = 12;
 // chi2 into d_chi2; d_v == nullptr: beta = J^T W (y_obs - y) into d_out,

@@ -865,7 +865,9 @@ int ps_fit(ps_ctx* c, double freq, int pole, ps_fit_result* out, double* cg_out)
     out->chisq = o.chisq;
     out->niter = o.niter;
     out->status = o.status;
-    (void)cg_out;
+    // a single fit leaves its final parameters at the start of its CTA's scratch
+    if (cg_out)
+        PSB_CUDA(cudaMemcpy(cg_out, c->d_scratch.p, (size_t)c->dp.ma * sizeof(double), cudaMemcpyDeviceToHost));
     return PS_OK;
 }
 
@@ -964,6 +966,208 @@ int ps_chi2_grad(ps_ctx* c, const double* a, double* chi2, double* beta) {
 int ps_gn_product(ps_ctx* c, const double* a, const double* v, double* out) {
     if (!v) return fail(PS_ERR_ARG, "null direction vector");
     return run_adjoint(c, a, v, nullptr, out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Gauss-Jordan solve of a x = b (a n x n row-major, overwritten; b becomes
+// x) with full pivoting as gauss_errc does it: the pivot is the last element
+// of largest magnitude in row-major order among the rows and columns not yet
+// used (a NaN never wins).  Returns 0, 1 when no pivot can be found, 2 on a
+// zero pivot (the reference's error codes).
+int host_gauss_jordan(std::vector<double>& a, std::vector<double>& b, int n) {
+    std::vector<int> used(n, 0);
+    for (int step = 0; step < n; step++) {
+        int prow = -1, pcol = -1;
+        double big = -1.0;
+        for (int j = 0; j < n; j++) {
+            if (used[j]) continue;
+            for (int k = 0; k < n; k++) {
+                if (used[k]) continue;
+                const double m = std::fabs(a[(size_t)j * n + k]);
+                if (m >= big) {  // NaN compares false
+                    big = m;
+                    prow = j;
+                    pcol = k;
+                }
+            }
+        }
+        if (prow < 0) return 1;
+        used[pcol] = 1;
+        if (prow != pcol) {
+            for (int l = 0; l < n; l++) std::swap(a[(size_t)prow * n + l], a[(size_t)pcol * n + l]);
+            std::swap(b[prow], b[pcol]);
+        }
+        const double piv = a[(size_t)pcol * n + pcol];
+        if (piv == 0.0) return 2;
+        const double inv = 1.0 / piv;
+        a[(size_t)pcol * n + pcol] = 1.0;
+        for (int l = 0; l < n; l++) a[(size_t)pcol * n + l] *= inv;
+        b[pcol] *= inv;
+        for (int r = 0; r < n; r++) {
+            if (r == pcol) continue;
+            const double f = a[(size_t)r * n + pcol];
+            a[(size_t)r * n + pcol] = 0.0;
+            for (int l = 0; l < n; l++) a[(size_t)r * n + l] -= a[(size_t)pcol * n + l] * f;
+            b[r] -= b[pcol] * f;
+        }
+    }
+    return 0;
+}
+
+// Device buffers of a Jacobian-free fit, carved from d_adj.
+struct JfreeBufs {
+    double *work, *a, *units, *alpha, *beta, *chi2;
+};
+
+JfreeBufs jfree_bufs(ps_ctx* c) {
+    const psb::DevProblem& d = c->dp;
+    JfreeBufs B;
+    B.work = c->d_adj.p;
+    B.a = B.work + psb::adjoint_work_doubles(d);
+    B.units = B.a + d.ma;
+    B.alpha = B.units + (size_t)d.mfit * d.ma;
+    B.beta = B.alpha + (size_t)d.mfit * d.mfit;
+    B.chi2 = B.beta + d.mfit;
+    return B;
+}
+
+// One evaluation at a through the matrix-free kernels: chi2, chck, the
+// facet-area sum and, with full, beta and alpha (alpha's column k is the
+// Gauss-Newton product with the k-th free unit vector, mfit products).
+int jfree_eval(ps_ctx* c, const JfreeBufs& B, const double* a, bool full, std::vector<double>& alpha,
+               std::vector<double>& beta, double* scal) {
+    const psb::DevProblem& d = c->dp;
+    const int mfit = d.mfit, ma = d.ma;
+    PSB_CUDA(cudaMemcpyAsync(B.a, a, ma * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    PSB_CUDA(psb::launch_adjoint(d, c->d_dp.p, B.work, B.a, nullptr, B.beta, B.chi2, c->stream));
+    for (int k = 0; k < psb::kAdjointLaunches; k++) psb::count_launch();
+    // chck and the area sum depend on a only: read them before the products
+    const double* misc = B.work + psb::adjoint_misc_offset(d);
+    PSB_CUDA(cudaMemcpyAsync(scal + 1, misc + psb::kAdjMiscChk, 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PSB_CUDA(cudaMemcpyAsync(scal + 4, misc + psb::kAdjMiscSarea, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    PSB_CUDA(cudaMemcpyAsync(scal, B.chi2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (full) {
+        for (int k = 0; k < mfit; k++) {
+            PSB_CUDA(psb::launch_adjoint(d, c->d_dp.p, B.work, B.a, B.units + (size_t)k * ma,
+                                         B.alpha + (size_t)k * mfit, B.chi2 + 1, c->stream));
+            for (int q = 0; q < psb::kAdjointLaunches; q++) psb::count_launch();
+        }
+        std::vector<double> cols((size_t)mfit * mfit);
+        PSB_CUDA(cudaMemcpyAsync(cols.data(), B.alpha, cols.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                 c->stream));
+        beta.resize(mfit);
+        PSB_CUDA(cudaMemcpyAsync(beta.data(), B.beta, mfit * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        PSB_CUDA(cudaStreamSynchronize(c->stream));
+        // alpha[j][k] for k <= j from column k, mirrored (alpha is symmetric)
+        alpha.assign((size_t)mfit * mfit, 0.0);
+        for (int k = 0; k < mfit; k++)
+            for (int j = k; j < mfit; j++) {
+                const double v = cols[(size_t)k * mfit + j];
+                alpha[(size_t)j * mfit + k] = v;
+                alpha[(size_t)k * mfit + j] = v;
+            }
+    } else {
+        PSB_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return PS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ps_fit_jfree(ps_ctx* c, double freq, int pole, ps_fit_result* out, double* cg_out) {
+    int rc = check_ready(c, true);
+    if (rc) return rc;
+    if (pole < 1 || pole > 10 || !(freq > 0) || !out) return fail(PS_ERR_ARG, "bad fit arguments");
+    PSB_CUDA(cudaSetDevice(c->device));
+    const psb::DevProblem& d = c->dp;
+    const int ma = d.ma, mfit = d.mfit, C = d.C;
+    PSB_CUDA(c->d_adj.ensure(psb::adjoint_work_doubles(d) + (size_t)ma + (size_t)mfit * ma + (size_t)mfit * mfit +
+                             mfit + 2));
+    const JfreeBufs B = jfree_bufs(c);
+    {
+        std::vector<double> units((size_t)mfit * ma, 0.0);
+        for (int k = 0; k < mfit; k++) units[(size_t)k * ma + c->free_idx[k]] = 1.0;
+        PSB_CUDA(cudaMemcpyAsync(B.units, units.data(), units.size() * sizeof(double), cudaMemcpyHostToDevice,
+                                 c->stream));
+        PSB_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    std::vector<double> cg(ma), atry(ma), alpha, beta, covar, da;
+    psb::initial_parameters(c->prob, freq, pole, cg.data());
+    double scal[5];
+    // the LM loop and stop rule of the fit kernels (period_search_BOINC.cpp:846-920,
+    // mrqmin.c:11-110)
+    double alamda = -1, ochisq = 0, chisq = 0, iter_diff = 1e40, dev_old = 1e30, dev_new = 0, rchisq = -1;
+    double chk[3] = {0, 0, 0}, cur[3] = {0, 0, 0}, s_cur = 0, s_last = 0;
+    int niter = 0, status = 0;
+    bool j_stale = false;
+    while (((niter < d.n_iter_max) && (iter_diff > d.iter_diff_max)) || (niter < d.n_iter_min)) {
+        if (alamda < 0) {
+            alamda = d.alamda_start;
+            rc = jfree_eval(c, B, cg.data(), true, alpha, beta, scal);
+            if (rc) return rc;
+            ochisq = scal[0];
+            for (int i = 0; i < 3; i++) cur[i] = scal[1 + i];
+            s_cur = s_last = scal[4];
+            atry = cg;
+        } else if (j_stale) {
+            rc = jfree_eval(c, B, cg.data(), true, alpha, beta, scal);
+            if (rc) return rc;
+            j_stale = false;
+        }
+        covar = alpha;
+        for (int j = 0; j < mfit; j++) covar[(size_t)j * mfit + j] = alpha[(size_t)j * mfit + j] * (1 + alamda);
+        da = beta;
+        const int err = host_gauss_jordan(covar, da, mfit);
+        if (err == 0) {
+            for (int j = 0; j < mfit; j++) atry[c->free_idx[j]] = cg[c->free_idx[j]] + da[j];
+            rc = jfree_eval(c, B, atry.data(), false, alpha, beta, scal);
+            if (rc) return rc;
+            chisq = scal[0];
+            s_last = scal[4];
+            if (chisq < ochisq) {
+                alamda = alamda / d.alamda_incr;
+                j_stale = true;
+                cg = atry;
+                for (int i = 0; i < 3; i++) cur[i] = scal[1 + i];
+                s_cur = scal[4];
+            } else {
+                alamda = d.alamda_incr * alamda;
+                chisq = ochisq;
+            }
+        } else {
+            if (status == 0) status = err;
+            if (niter == 0) chisq = ochisq;
+        }
+        niter++;
+        if ((niter == 1) || (chisq < ochisq)) {
+            ochisq = chisq;
+            for (int i = 0; i < 3; i++) chk[i] = cur[i];
+            s_last = s_cur;
+            rchisq = chisq - (chk[0] * chk[0] + chk[1] * chk[1] + chk[2] * chk[2]) * (d.conw_r * d.conw_r);
+        }
+        dev_new = std::sqrt(rchisq / d.ndata_m3);
+        if (dev_old - dev_new > 1e-10) {
+            iter_diff = dev_old - dev_new;
+            dev_old = dev_new;
+        }
+    }
+    const double kPi = 3.14159265358979323846;
+    out->dev = dev_new;
+    out->dark = std::sqrt(chk[0] * chk[0] + chk[1] * chk[1] + chk[2] * chk[2]);
+    out->totarea = s_last;
+    out->period_d = 2 * kPi / cg[C + 2];
+    out->lambda_deg = (180 / kPi) * cg[C + 1];
+    out->beta_deg = 90 - (180 / kPi) * cg[C];
+    out->chisq = chisq;
+    out->niter = niter;
+    out->status = status;
+    if (cg_out) std::memcpy(cg_out, cg.data(), (size_t)ma * sizeof(double));
+    return PS_OK;
 }
 
 int ps_model(ps_ctx* c, const double* a, double* ymod, double* dyda) {

@@ -1331,6 +1331,10 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
             o.end_us = (unsigned int)(t_end / 1000ull);
             Bt.out[w] = o;
         }
+        // a single fit (ps_fit) leaves its final parameters at the start of
+        // the CTA's scratch, which no thread reads any more
+        if (Bt.pole_override)
+            for (int i = tid; i < ma; i += kThreads) Jt[i] = cg[i];
     }
 }
 

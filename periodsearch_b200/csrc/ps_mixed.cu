@@ -802,6 +802,10 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
             o.end_us = (unsigned int)(t_end / 1000ull);
             Bt.out[w] = o;
         }
+        // a single fit (ps_fit) leaves its final parameters at the start of
+        // the CTA's scratch, which no thread reads any more
+        if (Bt.pole_override)
+            for (int i = tid; i < ma; i += kThreads) Bt.scratch[(size_t)blockIdx.x * Bt.scratch_stride + i] = cg[i];
     }
     tmem_teardown(Parr[0], smem_raw, tmem);
 }
