@@ -112,8 +112,9 @@ __device__ __forceinline__ void point_geometry(const DevProblem& P, int p, const
     }
 }
 
-// Words of shared memory gauss_jordan needs in buf for an n x n system.
-__host__ __device__ constexpr int gj_buf_doubles(int n) { return 3 * n + 4 + 4 * (kThreads / 32); }
+// Words of shared memory gauss_jordan (and solve_spd) need in buf for an
+// n x n system.
+__host__ __device__ constexpr int gj_buf_doubles(int n) { return 4 * n + 4 + 4 * (kThreads / 32); }
 
 // Register tile of gauss_jordan for systems of at most nmax unknowns: rows
 // warp + 8 r (r < kR), columns lane + 32 c (c < kC), column n standing for b.
@@ -285,6 +286,95 @@ __device__ int gauss_jordan(double* a, double* b, int n, double* buf) {
             }
         }
         candidate(bk, bi);
+    }
+#pragma unroll
+    for (int r = 0; r < kR; r++)
+#pragma unroll
+        for (int c = 0; c < kC; c++) {
+            const int j = warp + kW * r, l = lane + 32 * c;
+            if (j < n && l == n) b[j] = x[r][c];
+        }
+    __syncthreads();
+    return 0;
+}
+
+// Solve a x = b for a symmetric positive definite n x n row-major matrix a
+// (shared memory, n <= nmax <= 96; the damped alpha of an LM step, alpha with
+// its diagonal times 1 + lambda) by Gauss-Jordan elimination with the
+// diagonal as pivots, in order: no pivot search, one block barrier per step.
+// The solution replaces b.  Returns 0, or -1 as soon as a pivot is not
+// above kSpdPivot times its original diagonal entry (a singular, nearly
+// singular or indefinite system, or NaN), leaving a and b untouched, so that
+// the caller runs gauss_jordan, the reference's full-pivot solve, for those:
+// there the pivot order decides the solution's ill-determined directions
+// and the singular verdict.  Same register tile as gauss_jordan; per step the owners publish
+// the pivot row and the pivot column to alternating halves of buf.
+constexpr double kSpdPivot = 1e-3;
+template <int nmax>
+__device__ int solve_spd(const double* a, double* b, int n, double* buf) {
+    using T = GjTile<nmax>;
+    constexpr int kW = T::kW, kR = T::kR, kC = T::kC;
+    static_assert(nmax <= 96 && kR <= 32 && kC <= 32, "tile");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double x[kR][kC];
+#pragma unroll
+    for (int r = 0; r < kR; r++) {
+        const int j = warp + kW * r;
+#pragma unroll
+        for (int c = 0; c < kC; c++) {
+            const int l = lane + 32 * c;
+            x[r][c] = (j < n && l <= n) ? (l < n ? a[j * n + l] : b[j]) : 0.0;
+        }
+    }
+    for (int i = 0; i < n; i++) {
+        double* prow = buf + (i & 1) * (2 * n + 2);  // row i, [n] = b_i
+        double* colv = prow + n + 1;                 // column i
+        if ((i & (kW - 1)) == warp) {
+            const int ri = i / kW;
+#pragma unroll
+            for (int r = 0; r < kR; r++)
+                if (r == ri) {
+#pragma unroll
+                    for (int c = 0; c < kC; c++)
+                        if (lane + 32 * c <= n) prow[lane + 32 * c] = x[r][c];
+                }
+        }
+        if ((i & 31) == lane) {
+            const int ci = i >> 5;
+#pragma unroll
+            for (int c = 0; c < kC; c++)
+                if (c == ci) {
+#pragma unroll
+                    for (int r = 0; r < kR; r++)
+                        if (warp + kW * r < n) colv[warp + kW * r] = x[r][c];
+                }
+        }
+        __syncthreads();
+        const double piv = prow[i];
+        if (!(piv > kSpdPivot * a[i * n + i])) {  // the same value in every thread
+            __syncthreads();  // nobody reads buf any more when the caller reuses it
+            return -1;
+        }
+        const double pivinv = 1.0 / piv;
+        double pr[kC];
+#pragma unroll
+        for (int c = 0; c < kC; c++) {
+            const int l = lane + 32 * c;
+            pr[c] = l <= n ? prow[l] * pivinv : 0.0;
+        }
+#pragma unroll
+        for (int r = 0; r < kR; r++) {
+            const int j = warp + kW * r;
+            if (j >= n) continue;
+            if (j == i) {
+#pragma unroll
+                for (int c = 0; c < kC; c++) x[r][c] = pr[c];
+            } else {
+                const double dum = colv[j];
+#pragma unroll
+                for (int c = 0; c < kC; c++) x[r][c] = x[r][c] - pr[c] * dum;
+            }
+        }
     }
 #pragma unroll
     for (int r = 0; r < kR; r++)

@@ -1268,7 +1268,11 @@ __global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_ke
             }
             for (int j = tid; j < mfit; j += kThreads) da[j] = beta[j];
             __syncthreads();
-            const int err = gauss_jordan<NCB + 8>(covar, da, mfit, sm + L.work);
+            // the fast form solves the damped system (symmetric positive
+            // definite unless singular) without pivot search; the full-pivot
+            // solve decides the cases that fails on, as in the reference
+            int err = kFast ? solve_spd<NCB + 8>(covar, da, mfit, sm + L.work) : -1;
+            if (err < 0) err = gauss_jordan<NCB + 8>(covar, da, mfit, sm + L.work);
             __syncthreads();
             if (err == 0) {
                 for (int j = tid; j < mfit; j += kThreads) {
