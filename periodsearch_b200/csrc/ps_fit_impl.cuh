@@ -63,6 +63,7 @@ __host__ __device__ constexpr int gj_covar_off(int mfit) { return (gj_buf_double
 // Shared-memory layout, offsets in doubles.
 struct Layout {
     int cg, atry, alpha, beta, da, g, area, dres, dave, blm, misc, red, perm, work, ipiv, ent;
+    int wlen;  // doubles of the work area
     size_t bytes;
 };
 
@@ -100,6 +101,7 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     if (gj_covar_off(P.mfit) + P.mfit * P.mfit > w) w = gj_covar_off(P.mfit) + P.mfit * P.mfit;
     PSB_TAKE(perm, P.sortseg / 2)
     PSB_TAKE(work, w)
+    L.wlen = w;
 #undef PSB_TAKE
     L.ipiv = o;
     L.ent = o + (P.mfit + 2 + 1) / 2;  // int offset counted in doubles
@@ -800,13 +802,18 @@ __device__ void model_pass(const DevProblem& P, const double* a, double* g, doub
     __syncthreads();
 }
 
+// The model rows go to the work area past the sort keys and the staged
+// normals when they fit there (nothing reads them after the pass but its own
+// normalisation and chi2), else to yt in global memory.
 template <int NCB, bool kFast>
 __device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, int a_off, double* yt) {
     extern __shared__ __align__(16) double sm[];
     const DevProblem& P = *Pp;
     const Layout L = make_layout(P);
+    const int yoff = P.sortseg > 4 * kMf ? P.sortseg : 4 * kMf;
+    double* ym = yoff + P.npad <= L.wlen ? sm + L.work + yoff : yt;
     model_pass<kFast>(P, sm + a_off, sm + L.g, sm + L.area, sm + L.misc, sm + L.blm, sm + L.blm + 9, sm + L.work,
-                      (int*)(sm + L.perm), yt);
+                      (int*)(sm + L.perm), ym);
 }
 
 template <int NCB, bool kFast>

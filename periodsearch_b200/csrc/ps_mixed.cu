@@ -555,7 +555,8 @@ __device__ __noinline__ void evaluate_mixed(const DevProblem* __restrict__ Pp, u
 
 // The model alone at a trial point (fitimpl::model_pass: FP64, the fast
 // form's arithmetic), with the operand-tile region -- idle between
-// evaluations -- as its g, work and perm buffers.
+// evaluations -- as its g, work and perm buffers and, when they fit, its
+// model rows (nothing reads them after the pass), else yt.
 __device__ __noinline__ void evaluate_model_mixed(const DevProblem* __restrict__ Pp, uint8_t* raw, const double* a,
                                                   double* yt) {
     const DevProblem& P = *Pp;
@@ -565,7 +566,10 @@ __device__ __noinline__ void evaluate_model_mixed(const DevProblem* __restrict__
     const size_t work_off = (((size_t)P.F * 8) + 255) & ~(size_t)255;
     double* work = (double*)(M.base + work_off);
     int* perm = (int*)(M.base + work_off + (size_t)model_work_doubles(P) * 8);
-    fitimpl::model_pass<true>(P, a, g, M.d(L.area), M.d(L.misc), M.d(L.blm), M.d(L.blm) + 9, work, perm, yt);
+    const size_t y_off = (work_off + (size_t)model_work_doubles(P) * 8 + (size_t)P.sortseg * 4 + 15) & ~(size_t)15;
+    double* ym = y_off + (size_t)P.npad * 8 <= (size_t)(4 * kTileP * 128 + 4 * kNc * 128) ? (double*)(M.base + y_off)
+                                                                                           : yt;
+    fitimpl::model_pass<true>(P, a, g, M.d(L.area), M.d(L.misc), M.d(L.blm), M.d(L.blm) + 9, work, perm, ym);
 }
 
 __device__ void tmem_setup(const DevProblem& P, uint8_t* raw, uint32_t* tmem) {
@@ -742,7 +746,9 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
             }
             for (int j = tid; j < mfit; j += kThreads) da[j] = beta[j];
             __syncthreads();
-            const int err = gauss_jordan<72>(covar, da, mfit, M.d(L.gwork));
+            // as in the fast FP64 form: diagonal pivots, full pivoting where they fail
+            int err = solve_spd<72>(covar, da, mfit, M.d(L.gwork));
+            if (err < 0) err = gauss_jordan<72>(covar, da, mfit, M.d(L.gwork));
             __syncthreads();
             if (err == 0) {
                 for (int j = tid; j < mfit; j += kThreads) {
