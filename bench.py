@@ -702,7 +702,12 @@ def main():
             e2e_times.append(t4 - t0)
             for k, dt in zip(phases, (t1 - t0, t2 - t1, t3 - t2, t4 - t3)):
                 phases[k].append(dt)
-    e2e_value = world * fits_per_step * len(e2e_times) / sum(e2e_times) if e2e_times else None
+    e2e_sum = sum(e2e_times)
+    if dist and e2e_times:
+        t_e2e = torch.tensor([e2e_sum], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)  # the slowest rank, as for the device time
+        e2e_sum = float(t_e2e.item())
+    e2e_value = world * fits_per_step * len(e2e_times) / e2e_sum if e2e_times else None
     same = times[:len(e2e_times)]
     e2e_extra = {"device_same_batches": world * fits_per_step * len(same) / sum(same) if same else None,
                  "phase_ms_median": {k: 1000 * statistics.median(v) for k, v in phases.items() if v},
