@@ -39,8 +39,9 @@ enum {
 /* Numerical form of the fit kernels. */
 enum {
     PS_FORM_FP64 = 0, /* plain FP64, reference operation order (the drop-in) */
-    PS_FORM_MIXED = 1, /* FP64 model/chi2/solve, FP32 derivatives, shape block of
-                          the Jacobian on the tensor cores (split BF16) */
+    PS_FORM_MIXED = 1, /* FP64 model/chi2/beta/solve, FP32 derivatives, shape block
+                          of the Jacobian (split BF16) and alpha (split TF32) on
+                          the tensor cores */
     PS_FORM_FAST = 2   /* FP64 throughout, derivative work rearranged and fused
                           (rounding-level differences to PS_FORM_FP64) */
 };

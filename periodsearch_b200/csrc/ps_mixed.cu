@@ -24,8 +24,9 @@
 // mbarrier; operand tiles are double-buffered so the next chunk's SIMT work
 // overlaps the tensor core.  Y chunks are stored pre-split and pre-swizzled
 // in HBM (built once per asteroid) and copied to shared memory per chunk.
-// alpha = J^T W J is accumulated in FP32 (it only shapes the step, not the
-// fixed point); beta and chi2 in FP64.  Every mbarrier wait is bounded; a
+// alpha = J^T W J runs on the tensor cores too (kind::tf32, split TF32,
+// FP32 accumulation: it only shapes the step, not the fixed point); beta and
+// chi2 in FP64 on the SIMT pipes.  Every mbarrier wait is bounded; a
 // wait that gives up sets the device error word, which the host reports.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -46,8 +47,7 @@ using namespace fitcommon;
 constexpr int kTileP = 128;     // points per tile (MMA M)
 constexpr int kKc = 64;         // facets per chunk (one swizzled 128-byte row)
 constexpr int kNc = 64;         // MMA N (shape coefficients, C <= 64)
-constexpr int kRtM = 32;        // rows per alpha tile
-constexpr int kMaxEptM = 16;    // alpha/beta/chi2 entries per thread
+constexpr int kRtM = 32;        // rows per alpha chunk (one 128-byte FP32 K row)
 // Bounded waits: the ordinary waits on the tensor core take P.max_polls
 // polls at most (ps_open sets it, by default kMaxPolls); a wait that gives up
 // ends the fit: the CTA stops taking work, waits for its own MMAs in flight
@@ -66,7 +66,7 @@ struct MLayout {
     uint32_t flt;                                 // byte offset of the float region
     int area32, dga32;                            // float offsets
     uint32_t ints;                                // byte offset of the int region
-    int ipiv, ent;                                // int offsets
+    int ipiv;                                     // int offsets
     size_t bytes;                                 // total incl. 1024 B alignment slack
 };
 
@@ -94,8 +94,7 @@ __host__ __device__ inline MLayout make_mlayout(const DevProblem& P) {
         L.b_lo[b] = o;
         o += kNc * 128;
     }
-    // the alpha tile (FP32) reuses the operand region after the point loop:
-    // kRtM x (mfit + 1) + kRtM x mfit floats, well inside 96 KB
+    // the alpha chunks (split TF32) reuse the operand buffers after the point loop
     L.mbar = o;
     o += 32;
     // TMEM base address, then the work item and asteroid of the current fit
@@ -123,7 +122,7 @@ __host__ __device__ inline MLayout make_mlayout(const DevProblem& P) {
     PSB_TAKE(blm, 28)
     PSB_TAKE(misc, 32)
     PSB_TAKE(red, 2 * (kThreads / 32) + 2)
-    PSB_TAKE(gwork, gj_buf_doubles(P.mfit) > 2 * kRtM ? gj_buf_doubles(P.mfit) : 2 * kRtM)
+    PSB_TAKE(gwork, gj_buf_doubles(P.mfit) > 3 * kRtM ? gj_buf_doubles(P.mfit) : 3 * kRtM)  // solve; alpha rows
 #undef PSB_TAKE
     o += (uint32_t)d * 8;
     L.flt = o;
@@ -135,9 +134,7 @@ __host__ __device__ inline MLayout make_mlayout(const DevProblem& P) {
     o += (uint32_t)f * 4;
     L.ints = o;
     L.ipiv = 0;
-    L.ent = (P.mfit + 3) & ~3;
-    const int nent = P.mfit * (P.mfit + 1) / 2 + P.mfit + 1;
-    o += (uint32_t)(L.ent + nent) * 4;
+    o += (uint32_t)((P.mfit + 3) & ~3) * 4;
     L.bytes = (size_t)o + 1024;
     return L;
 }
@@ -197,7 +194,6 @@ __device__ __noinline__ void evaluate_mixed(const DevProblem* __restrict__ Pp, u
     float* area32 = M.flt + L.area32;
     float* dga32 = M.flt + L.dga32;
     uint64_t* mbar = (uint64_t*)(M.base + L.mbar);
-    const int* ent = M.ints + L.ent;
     uint32_t gc = *gc_io;
     bool aborted = false;
 
@@ -481,72 +477,149 @@ __device__ __noinline__ void evaluate_mixed(const DevProblem* __restrict__ Pp, u
         }
         __syncthreads();
     }
-    // alpha (FP32 products, FP32 accumulation), beta and chi2 (FP64)
+    // alpha = J^T W J on the tensor cores (kind::tf32 with split-TF32
+    // operands: hi*hi + hi*lo + lo*hi, FP32 accumulation in TMEM), kRtM = 32
+    // rows per chunk (one 128-byte K row of FP32): A = the free parameters'
+    // rows of (J w)^T, zero past mfit (M = 128), B = those of J^T (N = 64),
+    // both K-major over the chunk's rows, in the point loop's operand buffers
+    // and TMEM columns and with its mbarrier protocol.  beta and chi2 stay FP64
+    // on the SIMT pipes: the thread that stages an item (a parameter and 4
+    // rows) accumulates its share of beta, the item sums of a parameter are
+    // added in a fixed order at the end; chi2 is summed in row order by one
+    // thread.
     {
-        float* Ws = (float*)M.base;                 // [kRtM][mfit]  J sig2i w
-        float* Js = Ws + kRtM * mfit;               // [kRtM][mfit]  J
-        double* dyw = M.d(L.gwork);                 // [kRtM] dy sig2i w
-        double* dyv = dyw + kRtM;                   // [kRtM] dy
-        const int tri = mfit * (mfit + 1) / 2;
-        const int nent = tri + mfit + 1;
-        float accf[kMaxEptM];
-        double accd[kMaxEptM];
-#pragma unroll
-        for (int s = 0; s < kMaxEptM; s++) {
-            accf[s] = 0.f;
-            accd[s] = 0.0;
+        constexpr int nq = kRtM / 4;      // items per parameter and chunk
+        double* dyw = M.d(L.gwork);       // [kRtM] dy sig2i w
+        double* dyv = dyw + kRtM;         // [kRtM] dy
+        float* wf = (float*)(dyv + kRtM);  // [kRtM] sig2i w in FP32 (for A)
+        double* bpart = M.d(L.covar);     // [mfit][nq] item sums of beta (covar is free here)
+        const int nitems = mfit * nq;
+        double bacc[2] = {0.0, 0.0}, cacc = 0.0;
+        // rows past mfit are zero in every chunk: clear them once in both buffers
+        for (int b = 0; b < 2; b++) {
+            for (int i = tid; i < (kTileP - mfit) * 8; i += kThreads) {
+                const uint32_t o = (uint32_t)(mfit + (i >> 3)) * 128 + (uint32_t)(i & 7) * 16;
+                *(uint4*)(M.base + L.a_hi[b] + o) = make_uint4(0u, 0u, 0u, 0u);
+                *(uint4*)(M.base + L.a_lo[b] + o) = make_uint4(0u, 0u, 0u, 0u);
+            }
+            for (int i = tid; i < (kNc - mfit) * 8; i += kThreads) {
+                const uint32_t o = (uint32_t)(mfit + (i >> 3)) * 128 + (uint32_t)(i & 7) * 16;
+                *(uint4*)(M.base + L.b_hi[b] + o) = make_uint4(0u, 0u, 0u, 0u);
+                *(uint4*)(M.base + L.b_lo[b] + o) = make_uint4(0u, 0u, 0u, 0u);
+            }
         }
-        for (int r0 = 0; r0 < P.n_rows; r0 += kRtM) {
-            const int nr = min(kRtM, P.n_rows - r0);
-            __syncthreads();
-            for (int idx = tid; idx < nr * mfit; idx += kThreads) {
-                const int j = idx / nr, r = idx - j * nr;
-                const int row = r0 + r;
-                const float d = Jf[(size_t)P.free_idx[j] * npad + row];
-                Js[r * mfit + j] = d;
-                Ws[r * mfit + j] = d * (float)(P.sig2i[row] * P.wght[row]);
+        const uint32_t idesc_a = umma::idesc_tf32_f32(kTileP, kNc);
+        const int nch_a = (P.n_rows + kRtM - 1) / kRtM;
+        for (int ch = 0; ch < nch_a; ch++, gc++) {
+            const int buf = gc & 1, r0 = ch * kRtM;
+            bool fail = false;
+            if (tid == 0 && gc >= 2) fail = !umma::mbar_wait(&mbar[buf], ((gc - 2) >> 1) & 1, P.max_polls);
+            if (__syncthreads_or(fail)) {
+                aborted = true;
+                break;
             }
-            for (int r = tid; r < nr; r += kThreads) {
-                const int row = r0 + r;
-                const double dy = P.yobs[row] - yt[row];
-                dyv[r] = dy;
-                dyw[r] = dy * P.sig2i[row] * P.wght[row];
+            if (tid < kRtM) {
+                const int row = r0 + tid;
+                double dy = 0.0, dw = 0.0, w = 0.0;
+                if (row < P.n_rows) {
+                    dy = P.yobs[row] - yt[row];
+                    dw = dy * P.sig2i[row] * P.wght[row];
+                    w = P.sig2i[row] * P.wght[row];
+                }
+                dyv[tid] = dy;
+                dyw[tid] = dw;
+                wf[tid] = (float)w;
             }
             __syncthreads();
 #pragma unroll
-            for (int s = 0; s < kMaxEptM; s++) {
-                const int e = tid + s * kThreads;
-                if (e < tri) {
-                    const int pk = ent[e];
-                    const float* w = Ws + (pk & 0xffff);
-                    const float* jj = Js + (pk >> 16);
-                    float acc = accf[s];
-                    for (int r = 0; r < nr; r++) acc = fmaf(w[r * mfit], jj[r * mfit], acc);
-                    accf[s] = acc;
-                } else if (e < tri + mfit) {
-                    const float* jj = Js + (e - tri);
-                    double acc = accd[s];
-                    for (int r = 0; r < nr; r++) acc = fma((double)jj[r * mfit], dyw[r], acc);
-                    accd[s] = acc;
-                } else if (e < nent) {
-                    double acc = accd[s];
-                    for (int r = 0; r < nr; r++) acc = fma(dyv[r], dyw[r], acc);
-                    accd[s] = acc;
+            for (int s = 0; s < 2; s++) {
+                const int it = tid + s * kThreads;
+                if (it < nitems) {
+                    const int j = it / nq, rr = 4 * (it - j * nq);
+                    const float* src = Jf + (size_t)P.free_idx[j] * npad + r0 + rr;
+                    uint32_t ah[4], al[4], bh[4], bl[4];
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const float jv = r0 + rr + i < P.n_rows ? src[i] : 0.f;
+                        umma::split_tf32(jv * wf[rr + i], ah[i], al[i]);
+                        umma::split_tf32(jv, bh[i], bl[i]);
+                        bacc[s] = fma((double)jv, dyw[rr + i], bacc[s]);
+                    }
+                    const uint32_t o = umma::sw128_off32(j, rr);  // four consecutive rows: one 16-byte chunk
+                    *(uint4*)(M.base + L.a_hi[buf] + o) = make_uint4(ah[0], ah[1], ah[2], ah[3]);
+                    *(uint4*)(M.base + L.a_lo[buf] + o) = make_uint4(al[0], al[1], al[2], al[3]);
+                    *(uint4*)(M.base + L.b_hi[buf] + o) = make_uint4(bh[0], bh[1], bh[2], bh[3]);
+                    *(uint4*)(M.base + L.b_lo[buf] + o) = make_uint4(bl[0], bl[1], bl[2], bl[3]);
                 }
             }
-        }
+            if (tid == kThreads - 1)
+                for (int r = 0; r < kRtM; r++) cacc = fma(dyv[r], dyw[r], cacc);
+            umma::fence_proxy_async();
+            __syncthreads();
+            if (tid == 0) {
+                umma::fence_after_sync();
+                const uint32_t sa_hi = umma::smem_u32(M.base + L.a_hi[buf]);
+                const uint32_t sa_lo = umma::smem_u32(M.base + L.a_lo[buf]);
+                const uint32_t sb_hi = umma::smem_u32(M.base + L.b_hi[buf]);
+                const uint32_t sb_lo = umma::smem_u32(M.base + L.b_lo[buf]);
 #pragma unroll
-        for (int s = 0; s < kMaxEptM; s++) {
-            const int e = tid + s * kThreads;
-            if (e < tri) {
-                const int j = ent[e] & 0xffff, k = ent[e] >> 16;
-                alpha_out[j * mfit + k] = (double)accf[s];
-                alpha_out[k * mfit + j] = (double)accf[s];
-            } else if (e < tri + mfit) {
-                beta_out[e - tri] = accd[s];
-            } else if (e < nent) {
-                misc[M_CHISQ] = accd[s];
+                for (int kk = 0; kk < 4; kk++) {
+                    const uint32_t o = kk * 32;
+                    umma::mma_tf32(tmem, umma::desc_kmajor_sw128(sa_hi + o), umma::desc_kmajor_sw128(sb_hi + o),
+                                   idesc_a, (ch > 0 || kk > 0) ? 1u : 0u);
+                    umma::mma_tf32(tmem, umma::desc_kmajor_sw128(sa_hi + o), umma::desc_kmajor_sw128(sb_lo + o),
+                                   idesc_a, 1u);
+                    umma::mma_tf32(tmem, umma::desc_kmajor_sw128(sa_lo + o), umma::desc_kmajor_sw128(sb_hi + o),
+                                   idesc_a, 1u);
+                }
+                umma::commit(&mbar[buf]);
             }
+        }
+        if (!aborted) {
+#pragma unroll
+            for (int s = 0; s < 2; s++) {
+                const int it = tid + s * kThreads;
+                if (it < nitems) bpart[it] = bacc[s];
+            }
+            // the last chunk's MMAs (and with them all earlier ones) before the read-back
+            const uint32_t last = gc - 1;
+            bool fail = false;
+            if (tid == 0) fail = !umma::mbar_wait(&mbar[last & 1], (last >> 1) & 1, P.max_polls);
+            if (__syncthreads_or(fail)) aborted = true;
+        }
+        if (!aborted) {
+            umma::fence_after_sync();
+            if (tid < kTileP) {
+                // warps 0-3: TMEM lanes 32w..32w+31 hold parameter rows j
+                const int j = tid;
+                const uint32_t lane_base = (uint32_t)((tid >> 5) * 32) << 16;
+                float acc[16];
+#pragma unroll 1
+                for (int q4 = 0; q4 < kNc / 16; q4++) {
+                    umma::tmem_ld16(tmem + lane_base + q4 * 16, acc);
+                    if (j < mfit) {
+#pragma unroll
+                        for (int i = 0; i < 16; i++) {
+                            const int k = q4 * 16 + i;
+                            if (k <= j) {  // the lower triangle, mirrored: alpha exactly symmetric
+                                alpha_out[j * mfit + k] = (double)acc[i];
+                                alpha_out[k * mfit + j] = (double)acc[i];
+                            }
+                        }
+                    }
+                }
+            }
+            if (tid < mfit) {
+                double b = 0.0;
+                for (int q = 0; q < nq; q++) b += bpart[tid * nq + q];
+                beta_out[tid] = b;
+            }
+            if (tid == kThreads - 1) misc[M_CHISQ] = cacc;
+            umma::fence_before_sync();
+        } else if (tid == 0) {
+            atomicAdd(P.err, 1);
+            misc[M_CHISQ] = __longlong_as_double(0x7ff8000000000000ll);
+            misc[M_ABORT] = 1;
         }
     }
     *gc_io = gc;
@@ -622,7 +695,6 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
         qslot = (int*)(M0.base + M0.L.tslot) + 1;
     }
     uint32_t gc = 0;
-    int cur_mfit = -1;
     bool aborted = false;
 
     while (!aborted) {
@@ -665,10 +737,6 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_fit_kernel(const DevProblem
         double* cg = M.d(L.cg);
         double* atry = M.d(L.atry);
         double* misc = M.d(L.misc);
-        if (mfit != cur_mfit) {
-            entry_map(mfit, M.ints + L.ent);
-            cur_mfit = mfit;
-        }
         if (tid == 0) misc[M_ABORT] = 0;
         float* Jf = (float*)(Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride);
         double* yt = Bt.scratch + (size_t)blockIdx.x * Bt.scratch_stride + ((size_t)ma * P.npad + 1) / 2;
@@ -823,7 +891,6 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_eval_kernel(const DevProble
     const MLayout& L = M.L;
     const int tid = threadIdx.x;
     double* cg = M.d(L.cg);
-    entry_map(P.mfit, M.ints + L.ent);
     uint32_t tmem;
     tmem_setup(P, smem_raw, &tmem);
     uint32_t gc = 0;
@@ -844,7 +911,7 @@ __global__ void __launch_bounds__(kThreads, 1) mixed_eval_kernel(const DevProble
 }
 
 bool mixed_supported(const DevProblem& P) {
-    return P.C <= kNc && P.nchunk * kKc >= P.F && P.mfit * (P.mfit + 1) / 2 + P.mfit + 1 <= kMaxEptM * kThreads &&
+    return P.C <= kNc && P.nchunk * kKc >= P.F && P.mfit >= 8 && P.mfit <= kNc &&
            P.mfit <= 0xffff && P.bsw && P.fac32 && P.err &&
            ((((size_t)P.F * 8) + 255) & ~(size_t)255) + (size_t)model_work_doubles(P) * 8 + (size_t)P.sortseg * 4 <=
                (size_t)(4 * kTileP * 128 + 4 * kNc * 128);

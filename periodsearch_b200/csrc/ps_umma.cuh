@@ -40,6 +40,22 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N) {
            | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+// Instruction descriptor, kind::tf32 with TF32 A/B (FP32 storage, the top 19
+// bits used), FP32 D, both K-major.  A 128-byte K row holds 32 elements, one
+// MMA step (UMMA_K = 8) 32 bytes: the same descriptors and k-step offsets as
+// the BF16 tiles.
+__host__ __device__ constexpr uint32_t idesc_tf32_f32(int M, int N) {
+    return (1u << 4)                  // D format F32
+           | (2u << 7)                // A format TF32
+           | (2u << 10)               // B format TF32
+           | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// byte offset of element (r, k) in a K-major SW128 FP32 tile (32 wide)
+__device__ __forceinline__ uint32_t sw128_off32(int r, int k) {
+    return (uint32_t)(r * 128) + ((uint32_t)(4 * k) ^ ((uint32_t)(r & 7) << 4));
+}
+
 // byte offset of element (r, k) in a K-major SW128 BF16 tile (64 wide)
 __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
     return (uint32_t)(r * 128) + ((uint32_t)(2 * k) ^ ((uint32_t)(r & 7) << 4));
@@ -65,6 +81,14 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a_desc, uint6
     asm volatile(
         "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
         "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
 }
 
@@ -110,6 +134,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
         : "memory");
 #pragma unroll
     for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// FP32 -> (hi, lo) TF32 pair (FP32 bit patterns with the low 13 bits zero,
+// round to nearest) with x ~= hi + lo to ~2^-22 relative.
+__device__ __forceinline__ void split_tf32(float x, uint32_t& hi, uint32_t& lo) {
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(hi) : "f"(x));
+    const float r = x - __uint_as_float(hi);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(lo) : "f"(r));
 }
 
 // FP32 -> (hi, lo) BF16 pair with x ~= hi + lo to ~2^-16 relative.
