@@ -85,7 +85,9 @@ __host__ __device__ inline Layout make_layout(const DevProblem& P) {
     PSB_TAKE(blm, 28)
     PSB_TAKE(misc, 32)
     PSB_TAKE(red, 2 * (kThreads / 32) + 2)
-    int chunk = kFch * 5 + kFch * P.NCB;
+    // reference-order form: staged facets and g Dsph, then the rotation
+    // derivative vectors of the 128 points of a pass (18 doubles each)
+    int chunk = ((kFch * 5 + kFch * P.NCB + 1) & ~1) + 18 * (kThreads / 2);
     // fast form: two staged chunks, dsph rows padded to NCB + 4 doubles
     if (2 * P.fch * (8 + P.NCB) > chunk) chunk = 2 * P.fch * (8 + P.NCB);
     const int kB = (P.mfit + 1) & ~1;
@@ -816,6 +818,150 @@ __device__ __noinline__ void evaluate_model(const DevProblem* __restrict__ Pp, i
                       (int*)(sm + L.perm), ym);
 }
 
+// bright.c:54-125 for every data point in the reference's operation order
+// (PS_FORM_FP64), in segments of points sorted by viewing direction.  Two
+// threads per point: thread t works on point slot t mod 128 of a pass of 128
+// points, and its half h = t / 128 (warps 0-3, warps 4-7) keeps the shape
+// sums of coefficients [h NCB/2, (h + 1) NCB/2) and half of the other
+// per-point sums (h = 0: the brightness and the rotation derivatives 0 and 1;
+// h = 1: rotation derivative 2 and the two scattering sums).  Every sum runs
+// over the facets in order with the reference's operations, each in one
+// thread, so the results are the bits of one thread per point; both halves
+// form the per-pair terms (visibility, s, the derivative factors).  Each half
+// runs its own instantiation of the pass (H), so that a thread holds only its
+// half's state and its accumulators fit in 128 registers (two fits per SM);
+// both execute the same block barriers, warp by warp.
+template <int NCB, int H>
+__device__ __forceinline__ void ref_pass(const DevProblem& P, const double* B, const double* D, double* misc,
+                                         const double* g, const double* area, double* s_fac, double* s_dg,
+                                         double* sdv, int pl, bool act, int p, double* Jt, double* yt) {
+    constexpr int KH = NCB / 2;
+    constexpr int kPts = kThreads / 2;
+    const int tid = threadIdx.x;
+    const int F = P.F, C = P.C, npad = P.npad;
+    const double cl = misc[M_CL], cls = misc[M_CLS];
+    constexpr int c0 = H == 0 ? 0 : 2;  // the rotation derivative both halves keep
+    // this point's derivative vectors in shared memory ([vector][slot]: the
+    // loads of a warp are consecutive): H = 0 columns 0 and 1 of de, de0
+    // (12 doubles), H = 1 column 2 (6 doubles, after the 12 x 128 of H = 0)
+    double* dv = sdv + (H == 0 ? 0 : 12 * kPts) + pl;
+    double e[3] = {0, 0, 0}, e0[3] = {0, 0, 0};
+    if (act) {
+        PointGeom G;
+        point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+            e[i] = G.e[i];
+            e0[i] = G.e0[i];
+            dv[(0 + i) * kPts] = G.de[i][c0];
+            dv[(3 + i) * kPts] = G.de0[i][c0];
+            if constexpr (H == 0) {
+                dv[(6 + i) * kPts] = G.de[i][1];
+                dv[(9 + i) * kPts] = G.de0[i][1];
+            }
+        }
+    }
+    double acc[KH];
+#pragma unroll
+    for (int k = 0; k < KH; k++) acc[k] = 0;
+    double a0 = 0, a1 = 0, a2 = 0;  // H = 0: br, rot0, rot1; H = 1: s_cl, rot2, s_cls
+    for (int f0 = 0; f0 < F; f0 += kFch) {
+        const int nf = min(kFch, F - f0);
+        __syncthreads();
+        for (int idx = tid; idx < nf * NCB; idx += kThreads) {
+            const int ff = idx / NCB, k = idx - ff * NCB;
+            s_dg[idx] = g[f0 + ff] * P.dsph[(size_t)(f0 + ff) * NCB + k];
+        }
+        for (int ff = tid; ff < nf; ff += kThreads) {
+            const double* fa = P.fac + (size_t)(f0 + ff) * 4;
+            s_fac[ff * 5 + 0] = fa[0];
+            s_fac[ff * 5 + 1] = fa[1];
+            s_fac[ff * 5 + 2] = fa[2];
+            s_fac[ff * 5 + 3] = area[f0 + ff];
+            s_fac[ff * 5 + 4] = fa[3];
+        }
+        __syncthreads();
+        if (act) {
+            for (int ff = 0; ff < nf; ff++) {
+                const double nx = s_fac[ff * 5 + 0], ny = s_fac[ff * 5 + 1], nz = s_fac[ff * 5 + 2];
+                const double mu = e[0] * nx + e[1] * ny + e[2] * nz;
+                const double mu0 = e0[0] * nx + e0[1] * ny + e0[2] * nz;
+                if ((mu > kTinyD) && (mu0 > kTinyD)) {
+                    const double ar = s_fac[ff * 5 + 3], darea = s_fac[ff * 5 + 4];
+                    const double dnom = mu + mu0;
+                    const double s = mu * mu0 * (cl + cls / dnom);
+                    const double q0 = mu0 / dnom, q1 = mu / dnom;
+                    const double dsmu = cls * (q0 * q0) + cl * mu0;
+                    const double dsmu0 = cls * (q1 * q1) + cl * mu;
+                    const double dbr = darea * s;
+                    const double* dg = s_dg + ff * NCB + H * KH;
+#pragma unroll
+                    for (int k = 0; k < KH; k++) acc[k] = acc[k] + dbr * dg[k];
+                    {
+                        const double sum = nx * dv[0] + ny * dv[kPts] + nz * dv[2 * kPts];
+                        const double sum0 = nx * dv[3 * kPts] + ny * dv[4 * kPts] + nz * dv[5 * kPts];
+                        a1 = a1 + ar * (dsmu * sum + dsmu0 * sum0);
+                    }
+                    if constexpr (H == 0) {
+                        a0 = a0 + ar * s;
+                        const double sum = nx * dv[6 * kPts] + ny * dv[7 * kPts] + nz * dv[8 * kPts];
+                        const double sum0 = nx * dv[9 * kPts] + ny * dv[10 * kPts] + nz * dv[11 * kPts];
+                        a2 = a2 + ar * (dsmu * sum + dsmu0 * sum0);
+                    } else {
+                        a0 = a0 + mu * mu0 * ar;
+                        a2 = a2 + ar * mu * mu0 / (mu + mu0);
+                    }
+                }
+            }
+        }
+    }
+    if (act) {
+        PointGeom G;  // recomputed (the same values): no registers across the facet loop
+        point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
+        const double sc = G.scale;
+#pragma unroll
+        for (int k = 0; k < KH; k++)
+            if (H * KH + k < C) Jt[(size_t)(H * KH + k) * npad + p] = sc * acc[k];
+        if constexpr (H == 0) {
+            Jt[(size_t)(C + 0) * npad + p] = sc * a1;
+            Jt[(size_t)(C + 1) * npad + p] = sc * a2;
+            Jt[(size_t)(C + 3) * npad + p] = a0 * G.dphp[0];
+            Jt[(size_t)(C + 4) * npad + p] = a0 * G.dphp[1];
+            Jt[(size_t)(C + 5) * npad + p] = a0 * G.dphp[2];
+            yt[p] = a0 * sc;
+        } else {
+            Jt[(size_t)(C + 2) * npad + p] = sc * a1;
+            Jt[(size_t)(C + 6) * npad + p] = sc * a0 * cl;
+            Jt[(size_t)(C + 7) * npad + p] = sc * a2;
+        }
+    }
+}
+
+template <int NCB>
+__device__ __forceinline__ void point_loop_ref(const DevProblem& P, double* sm, const Layout& L, const double* B,
+                                               const double* D, double* misc, const double* g, const double* area,
+                                               double* work, double* Jt, double* yt) {
+    constexpr int kPts = kThreads / 2;
+    const int tid = threadIdx.x, h = tid / kPts, pl = tid - h * kPts;
+    double* s_fac = work;
+    double* s_dg = work + kFch * 5;
+    double* sdv = work + ((kFch * 5 + kFch * NCB + 1) & ~1);
+    int* perm = (int*)(sm + L.perm);
+    for (int s0 = 0; s0 < P.n_points; s0 += P.sortseg) {
+        const int seg = min(P.sortseg, P.n_points - s0);
+        __syncthreads();
+        sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
+        for (int base = 0; base < seg; base += kPts) {
+            const bool act = base + pl < seg;
+            const int p = act ? perm[base + pl] : 0;
+            if (h == 0)
+                ref_pass<NCB, 0>(P, B, D, misc, g, area, s_fac, s_dg, sdv, pl, act, p, Jt, yt);
+            else
+                ref_pass<NCB, 1>(P, B, D, misc, g, area, s_fac, s_dg, sdv, pl, act, p, Jt, yt);
+        }
+    }
+}
+
 template <int NCB, bool kFast>
 __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_off, int alpha_off, int beta_off,
                                       double* Jt, double* yt) {
@@ -873,141 +1019,7 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_o
             point_loop_fast<NCB, false>(P, sm, L, B, D, misc, g, area, dres, work, Jt, yt);
         }
     } else {
-        // bright.c:54-125 for every data point, in segments of points sorted by
-        // viewing direction
-        double* s_fac = work;
-        double* s_dg = work + kFch * 5;
-        int* perm = (int*)(sm + L.perm);
-        const double cl = misc[M_CL], cls = misc[M_CLS];
-        for (int s0 = 0; s0 < P.n_points; s0 += P.sortseg) {
-        const int seg = min(P.sortseg, P.n_points - s0);
-        __syncthreads();
-        sort_points(P, s0, seg, B, misc[M_OMG], (unsigned long long*)work, perm);
-        for (int base = 0; base < seg; base += kThreads) {
-            const bool act = base + tid < seg;
-            const int p = act ? perm[base + tid] : 0;
-            PointGeom G;
-            if (act) point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G);
-            double acc[NCB];
-    #pragma unroll
-            for (int k = 0; k < NCB; k++) acc[k] = 0;
-            double br = 0, rot0 = 0, rot1 = 0, rot2 = 0, s_cl = 0, s_cls = 0;
-            double sS0 = 0, sS1 = 0, sS2 = 0;  // kFast: sum Area dsmu0 n
-            for (int f0 = 0; f0 < F; f0 += kFch) {
-                const int nf = min(kFch, F - f0);
-                __syncthreads();
-                for (int idx = tid; idx < nf * NCB; idx += kThreads) {
-                    const int ff = idx / NCB, k = idx - ff * NCB;
-                    s_dg[idx] = g[f0 + ff] * P.dsph[(size_t)(f0 + ff) * NCB + k];
-                }
-                for (int ff = tid; ff < nf; ff += kThreads) {
-                    const double* fa = P.fac + (size_t)(f0 + ff) * 4;
-                    s_fac[ff * 5 + 0] = fa[0];
-                    s_fac[ff * 5 + 1] = fa[1];
-                    s_fac[ff * 5 + 2] = fa[2];
-                    s_fac[ff * 5 + 3] = area[f0 + ff];
-                    s_fac[ff * 5 + 4] = fa[3];
-                }
-                __syncthreads();
-                if (act) {
-                    for (int ff = 0; ff < nf; ff++) {
-                        const double nx = s_fac[ff * 5 + 0], ny = s_fac[ff * 5 + 1], nz = s_fac[ff * 5 + 2];
-                        const double mu = G.e[0] * nx + G.e[1] * ny + G.e[2] * nz;
-                        const double mu0 = G.e0[0] * nx + G.e0[1] * ny + G.e0[2] * nz;
-                        if ((mu > kTinyD) && (mu0 > kTinyD)) {
-                            const double ar = s_fac[ff * 5 + 3], darea = s_fac[ff * 5 + 4];
-                            if constexpr (kFast) {
-                                // one reciprocal; rotation derivatives through the
-                                // facet sums T = sum Area dsmu n, S = sum Area dsmu0 n
-                                const double r = 1.0 / (mu + mu0);
-                                const double s = mu * mu0 * fma(cls, r, cl);
-                                br = fma(ar, s, br);
-                                const double q0 = mu0 * r, q1 = mu * r;
-                                const double w = ar * fma(cls * q0, q0, cl * mu0);
-                                const double w0 = ar * fma(cls * q1, q1, cl * mu);
-                                rot0 = fma(w, nx, rot0);
-                                rot1 = fma(w, ny, rot1);
-                                rot2 = fma(w, nz, rot2);
-                                sS0 = fma(w0, nx, sS0);
-                                sS1 = fma(w0, ny, sS1);
-                                sS2 = fma(w0, nz, sS2);
-                                const double mm = mu * mu0 * ar;
-                                s_cl += mm;
-                                s_cls = fma(mm, r, s_cls);
-                                const double dbr = darea * s;
-                                const double* dg = s_dg + ff * NCB;
-    #pragma unroll
-                                for (int k = 0; k < NCB; k++) acc[k] = fma(dbr, dg[k], acc[k]);
-                            } else {
-                                const double dnom = mu + mu0;
-                                const double s = mu * mu0 * (cl + cls / dnom);
-                                br = br + ar * s;
-                                const double q0 = mu0 / dnom, q1 = mu / dnom;
-                                const double dsmu = cls * (q0 * q0) + cl * mu0;
-                                const double dsmu0 = cls * (q1 * q1) + cl * mu;
-                                const double dbr = darea * s;
-                                const double* dg = s_dg + ff * NCB;
-    #pragma unroll
-                                for (int k = 0; k < NCB; k++) acc[k] = acc[k] + dbr * dg[k];
-                                {
-                                    const double sum = nx * G.de[0][0] + ny * G.de[1][0] + nz * G.de[2][0];
-                                    const double sum0 = nx * G.de0[0][0] + ny * G.de0[1][0] + nz * G.de0[2][0];
-                                    rot0 = rot0 + ar * (dsmu * sum + dsmu0 * sum0);
-                                }
-                                {
-                                    const double sum = nx * G.de[0][1] + ny * G.de[1][1] + nz * G.de[2][1];
-                                    const double sum0 = nx * G.de0[0][1] + ny * G.de0[1][1] + nz * G.de0[2][1];
-                                    rot1 = rot1 + ar * (dsmu * sum + dsmu0 * sum0);
-                                }
-                                {
-                                    const double sum = nx * G.de[0][2] + ny * G.de[1][2] + nz * G.de[2][2];
-                                    const double sum0 = nx * G.de0[0][2] + ny * G.de0[1][2] + nz * G.de0[2][2];
-                                    rot2 = rot2 + ar * (dsmu * sum + dsmu0 * sum0);
-                                }
-                                s_cl = s_cl + mu * mu0 * ar;
-                                s_cls = s_cls + ar * mu * mu0 / (mu + mu0);
-                            }
-                        }
-                    }
-                }
-            }
-            if constexpr (kFast) {
-                // rotation derivatives from the facet-summed vectors; the point
-                // geometry is recomputed so that de/de0 need no registers in the loop
-                if (act) {
-                    PointGeom G2;
-                    point_geometry(P, p, B, D, misc[M_OMG], misc[M_P1], misc[M_P2], misc[M_P3], G2);
-                    const double T[3] = {rot0, rot1, rot2}, S[3] = {sS0, sS1, sS2};
-                    double rk[3];
-    #pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        double v = 0;
-    #pragma unroll
-                        for (int j = 0; j < 3; j++) v = fma(T[j], G2.de[j][k], fma(S[j], G2.de0[j][k], v));
-                        rk[k] = v;
-                    }
-                    rot0 = rk[0];
-                    rot1 = rk[1];
-                    rot2 = rk[2];
-                }
-            }
-            if (act) {
-                const double sc = G.scale;
-    #pragma unroll
-                for (int k = 0; k < NCB; k++)
-                    if (k < C) Jt[(size_t)k * npad + p] = sc * acc[k];
-                Jt[(size_t)(C + 0) * npad + p] = sc * rot0;
-                Jt[(size_t)(C + 1) * npad + p] = sc * rot1;
-                Jt[(size_t)(C + 2) * npad + p] = sc * rot2;
-                Jt[(size_t)(C + 3) * npad + p] = br * G.dphp[0];
-                Jt[(size_t)(C + 4) * npad + p] = br * G.dphp[1];
-                Jt[(size_t)(C + 5) * npad + p] = br * G.dphp[2];
-                Jt[(size_t)(C + 6) * npad + p] = sc * s_cl * cl;
-                Jt[(size_t)(C + 7) * npad + p] = sc * s_cls;
-                yt[p] = br * sc;
-            }
-        }
-        }
+        point_loop_ref<NCB>(P, sm, L, B, D, misc, g, area, work, Jt, yt);
     }
     __syncthreads();
     // convexity rows (conv.c:12-29): y = residual, J = dres for the shape
@@ -1138,7 +1150,7 @@ __device__ __noinline__ void evaluate(const DevProblem* __restrict__ Pp, int a_o
 }
 
 template <int NCB, bool kFast>
-__global__ void __launch_bounds__(kThreads, (kFast && NCB <= 64) ? 2 : 1) fit_kernel(const DevProblem* __restrict__ Parr, FitBatch Bt) {
+__global__ void __launch_bounds__(kThreads, NCB <= 64 ? 2 : 1) fit_kernel(const DevProblem* __restrict__ Parr, FitBatch Bt) {
     // No static __shared__ variable may be declared in these kernels: with
     // one, the dynamic region would start after it here but not in the
     // out-of-line evaluate(), which addresses it through its own extern
