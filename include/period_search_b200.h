@@ -174,7 +174,9 @@ int ps_scan_device_noalloc(ps_ctx* ctx, int n_from, int n_to, ps_record* d_out, 
  * nrows, and have conw_r settled (ps_precalc / ps_set_conw_r).  The batch
  * borrows the contexts' tables: close the batch before its contexts.  In
  * the mixed form ps_batch_scan reports a bounded device wait that gave up
- * as PS_ERR_DEVICE_LOOP (the fits it ended carry status -1). */
+ * as PS_ERR_DEVICE_LOOP (the fits it ended carry status -1); the
+ * asynchronous ps_batch_scan_device leaves that report to the next
+ * ps_batch_scan. */
 typedef struct ps_batch ps_batch;
 int ps_batch_open(ps_ctx* const* ctxs, int n, ps_batch** out);
 /* Scan periods n_from[a]..n_to[a] of every asteroid a; records are
