@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <tuple>
 
@@ -302,17 +303,24 @@ struct LuSolver {
 };
 
 // ellfit.c:11-88: Laplace-series coefficients of the ellipsoid's log
-// curvature function (normal equations + LU solve).
-int ellfit(Problem& p) {
+// curvature function (normal equations + LU solve).  The spherical-function
+// matrix, its normal matrix and that matrix's LU factors depend on the facet
+// grid alone (nrows, lmax, mmax): EllfitGrid holds them, built once per grid
+// and shared by every asteroid on it; per asteroid only the ellipsoid's log
+// radii, the right-hand side and the substitutions remain.  Every value is
+// formed by the same operations in the same order as in one pass, so the
+// coefficients are the same bits.
+struct EllfitGrid {
+    std::vector<double> fmat;  // [F][C]
+    LuSolver lu;
+    int rc = 0;  // 4: the normal matrix is singular (the reference's exit code)
+};
+
+std::shared_ptr<const EllfitGrid> ellfit_grid(const Problem& p) {
     const int F = p.numfac, C = p.ncoef, L1 = p.lmax + 1;
-    const double a = p.a_axis, b = p.b_axis, c = p.c_axis;
-    std::vector<double> er(F), fmat((size_t)F * C);
-    for (int i = 0; i < F; i++) {
-        double st = std::sin(p.at[i]);
-        double sum = std::pow(a * st * std::cos(p.af[i]), 2) + std::pow(b * st * std::sin(p.af[i]), 2) +
-                     std::pow(c * std::cos(p.at[i]), 2);
-        er[i] = 2 * (std::log(a * b * c) - std::log(sum));
-    }
+    auto eg = std::make_shared<EllfitGrid>();
+    std::vector<double>& fmat = eg->fmat;
+    fmat.assign((size_t)F * C, 0.0);
     for (int i = 0; i < F; i++) {
         int n = 0;
         for (int m = 0; m <= p.mmax; m++)
@@ -329,20 +337,35 @@ int ellfit(Problem& p) {
                 }
             }
     }
-    std::vector<double> fitmat((size_t)C * C), fitvec(C);
-    for (int i = 0; i < C; i++) {
+    std::vector<double> fitmat((size_t)C * C);
+    for (int i = 0; i < C; i++)
         for (int j = 0; j < C; j++) {
             double s = 0;
             for (int k = 0; k < F; k++) s = s + fmat[(size_t)k * C + i] * fmat[(size_t)k * C + j];
             fitmat[(size_t)i * C + j] = s;
         }
+    eg->rc = eg->lu.factor(fitmat, C);
+    return eg;
+}
+
+int ellfit(Problem& p, const EllfitGrid& eg) {
+    const int F = p.numfac, C = p.ncoef;
+    const double a = p.a_axis, b = p.b_axis, c = p.c_axis;
+    std::vector<double> er(F);
+    for (int i = 0; i < F; i++) {
+        double st = std::sin(p.at[i]);
+        double sum = std::pow(a * st * std::cos(p.af[i]), 2) + std::pow(b * st * std::sin(p.af[i]), 2) +
+                     std::pow(c * std::cos(p.at[i]), 2);
+        er[i] = 2 * (std::log(a * b * c) - std::log(sum));
+    }
+    if (eg.rc != 0) return 4;
+    std::vector<double> fitvec(C);
+    for (int i = 0; i < C; i++) {
         double s = 0;
-        for (int j = 0; j < F; j++) s = s + fmat[(size_t)j * C + i] * er[j];
+        for (int j = 0; j < F; j++) s = s + eg.fmat[(size_t)j * C + i] * er[j];
         fitvec[i] = s;
     }
-    LuSolver lu;
-    if (lu.factor(fitmat, C) != 0) return 4;
-    lu.solve(fitvec);
+    eg.lu.solve(fitvec);
     p.cg_first = fitvec;
     return 0;
 }
@@ -506,10 +529,11 @@ int finish_from_arrays(Problem& p, std::string& err) {
 // The facet grid and its spherical-harmonic tables (trifac, areanorm,
 // sphfunc) depend only on (nrows, lmax, mmax): computed once per process and
 // copied for every further asteroid on the same grid.
-void grid_tables(Problem& p) {
+std::shared_ptr<const EllfitGrid> grid_tables(Problem& p) {
     struct Tables {
         std::vector<int> ifp;
         std::vector<double> nor, darea, at, af, pleg, dsph, fc, fs;
+        std::shared_ptr<const EllfitGrid> ell;
     };
     static std::mutex mu;
     static std::map<std::tuple<int, int, int>, Tables> cache;
@@ -528,14 +552,17 @@ void grid_tables(Problem& p) {
             p.dsph = t.dsph;
             p.fc = t.fc;
             p.fs = t.fs;
-            return;
+            return t.ell;
         }
     }
     trifac(p.nrows, p.ifp);
     areanorm(p);
     sphfunc(p);
+    auto ell = ellfit_grid(p);
     std::lock_guard<std::mutex> lock(mu);
-    if (cache.size() < 16) cache.emplace(key, Tables{p.ifp, p.nor, p.darea, p.at, p.af, p.pleg, p.dsph, p.fc, p.fs});
+    if (cache.size() < 16)
+        cache.emplace(key, Tables{p.ifp, p.nor, p.darea, p.at, p.af, p.pleg, p.dsph, p.fc, p.fs, ell});
+    return ell;
 }
 
 int setup_geometry(Problem& p, std::string& err) {
@@ -549,8 +576,8 @@ int setup_geometry(Problem& p, std::string& err) {
     p.ndir = 4 * p.nrows * p.nrows + 2;
     p.nphpar = 3;
     p.ma = p.ncoef + 5 + p.nphpar;
-    grid_tables(p);
-    if (ellfit(p) != 0) {
+    const std::shared_ptr<const EllfitGrid> ell = grid_tables(p);
+    if (ellfit(p, *ell) != 0) {
         err = "singular matrix in the ellipsoid fit (ludcmp)";
         return 4;
     }

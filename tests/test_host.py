@@ -39,6 +39,12 @@ def test_host_setup_bitexact_vs_oracle(native, oracle_lib, name):
         a, b = o.array(arr), h.array(arr)
         assert a.shape == b.shape and np.array_equal(a, b), arr
     h.close()
+    # a second asteroid on the same facet grid takes the grid tables and the
+    # grid half of the ellipsoid fit from the per-process cache: same bits
+    h2 = native.PeriodSearch(path, host_only=True)
+    for arr in ("nor", "dsph", "cg_first"):
+        assert np.array_equal(o.array(arr), h2.array(arr)), arr
+    h2.close()
 
 
 def test_errors_are_status_codes(native, tmp_path):
