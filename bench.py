@@ -400,26 +400,36 @@ def c4_measure(args, local):
     # end to end through the public API: open every asteroid from its input
     # file (host setup and uploads on host threads), open the batch, scan the
     # step's periods into host records, close everything
-    e2e_times = []
+    e2e_times, phases = [], {"open_many": [], "batch_open": [], "scan": [], "close": []}
     h2d = sum(os.path.getsize(p) for p, _ in made)
     for s in range(0 if getattr(args, "no_e2e", False) else 1):
         a, b = ranges(args.warmup + s)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         cs = ps.open_many([p for p, _ in made], device=local, form=form, conw_r="start")
+        if tiles:  # the tile shapes the timed steps ran with
+            for c in cs:
+                c.set_tiles(*tiles)
+        t1 = time.perf_counter()
         bt = ps.PeriodSearchBatch(cs)
+        t2 = time.perf_counter()
         recs = bt.scan(a, b)
+        t3 = time.perf_counter()
         bt.close()
         for c in cs:
             c.close()
-        e2e_times.append(time.perf_counter() - t0)
+        t4 = time.perf_counter()
+        e2e_times.append(t4 - t0)
+        for k, dt in zip(phases, (t1 - t0, t2 - t1, t3 - t2, t4 - t3)):
+            phases[k].append(dt)
     if e2e_times:
         n_rec = sum(len(r) for r in recs)
         line["e2e"] = {"value": fits / args.steps * len(e2e_times) / sum(e2e_times), "unit": "fits/s",
                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(n_rec * 48),
                        "what": "per step: open all asteroids from their input files, open the batch (graph "
                                "capture), scan, records to host, close",
-                       "step_ms": [round(1000 * t, 1) for t in e2e_times]}
+                       "step_ms": [round(1000 * t, 1) for t in e2e_times],
+                       "phase_ms": {k: round(1000 * statistics.median(v), 1) for k, v in phases.items() if v}}
     return line
 
 
