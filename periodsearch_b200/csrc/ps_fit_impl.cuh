@@ -21,7 +21,7 @@ namespace {
 
 using namespace fitcommon;
 
-constexpr int kFch = 32;     // facets per shared-memory chunk (reference-order form)
+constexpr int kFch = 64;     // facets per shared-memory chunk (reference-order form)
 constexpr int kRt = 32;      // rows per alpha tile (reference-order form)
 constexpr int kMf = 128;     // facets per staged chunk of the model-only pass
 
