@@ -17,9 +17,11 @@
 //
 // Work split inside a CTA (256 threads):
 //   curv        thread per facet (facet areas, curv.c:10-38)
-//   bright      thread per data point, facets streamed through shared
-//               memory in chunks of kFch (bright.c:14-126), all sums kept in
-//               registers in facet order; Dg = g * Dsph built per chunk
+//   bright      two threads per data point, each holding half of the
+//               point's sums (every sum in one thread, in facet order),
+//               facets streamed through shared memory in chunks of kFch
+//               (bright.c:14-126); Dg = g * Dsph built per chunk; two CTAs
+//               (fits) per SM
 //   conv        thread per (row, coefficient), sequential over facets
 //               (conv.c:12-29)
 //   normalise   per relative lightcurve: thread per column for the sums,
