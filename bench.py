@@ -801,7 +801,7 @@ def main():
     # on the 300-fit profile launch of the c2 workload (bench.py --profile),
     # scaled to this launch's fits: the per-CTA J scratch (356 KB) stays in L2
     # at one fit per SM and is evicted at two
-    per_fit = {"fast": 2.50e7, "fp64": 5.20e6}.get(args.form) if args.config == "c2" else None
+    per_fit = {"fast": 2.50e7, "fp64": 1.83e7}.get(args.form) if args.config == "c2" else None
     if per_fit:
         roofline["traffic"] = per_fit * fits_per_step
         roofline["traffic_source"] = ("ncu dram bytes of the 300-fit c2 profile launch of this form, "
