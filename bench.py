@@ -799,8 +799,8 @@ def main():
                 "flop_rule": "per evaluation 2 N F C + N mfit (mfit + 1), 51 evaluations per fit"}
     # DRAM bytes per fit from ncu (dram__bytes_read.sum + dram__bytes_write.sum)
     # on the 300-fit profile launch of the c2 workload (bench.py --profile),
-    # scaled to this launch's fits: the per-CTA J scratch (356 KB) stays in L2
-    # at one fit per SM and is evicted at two
+    # scaled to this launch's fits: mostly the per-CTA J scratch (356 KB),
+    # written back from L2 at two fits per SM
     per_fit = {"fast": 2.50e7, "fp64": 1.83e7}.get(args.form) if args.config == "c2" else None
     if per_fit:
         roofline["traffic"] = per_fit * fits_per_step
