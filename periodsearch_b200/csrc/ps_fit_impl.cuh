@@ -882,6 +882,7 @@ __device__ __forceinline__ void ref_pass(const DevProblem& P, const double* B, c
         }
         __syncthreads();
         if (act) {
+#pragma unroll 2  // two facets in flight (1.9 % on c2; same operations per sum)
             for (int ff = 0; ff < nf; ff++) {
                 const double nx = s_fac[ff * 5 + 0], ny = s_fac[ff * 5 + 1], nz = s_fac[ff * 5 + 2];
                 const double mu = e[0] * nx + e[1] * ny + e[2] * nz;
